@@ -1,0 +1,165 @@
+/*
+ * patch_denoise_b200.h -- C ABI of the B200 (sm_100a) space-time low-rank
+ * denoising library (libpd_b200.so).
+ *
+ * The reference (paquiteau/patch-denoising) is pure Python; its hot path is the
+ * per-patch loop of BaseSpaceTimeDenoiser.denoise (src/patch_denoise/space_time/
+ * base.py:177-270) calling the per-method _patch_processing plug-ins
+ * (space_time/lowrank.py). These entry points replace that loop. Each one names
+ * the reference interface it stands in for. All buffers are caller-owned device
+ * memory (plain pointers + sizes); every call is asynchronous on the given stream
+ * unless its comment says it synchronises. No call throws: the status code says
+ * what went wrong and pd_last_error() gives a message.
+ *
+ * Data layout: a 4D volume (X, Y, Z, T) in C order (T fastest). Inputs of fewer
+ * spatial dimensions are padded with leading unit axes by pd_geometry_init.
+ * Complex volumes are interleaved float pairs (complex64).
+ */
+#ifndef PATCH_DENOISE_B200_H
+#define PATCH_DENOISE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t pd_status;
+#define PD_OK 0
+#define PD_ERR_INVALID 1     /* bad argument: the reference raises ValueError   */
+#define PD_ERR_UNSUPPORTED 2 /* valid but not handled by this build            */
+#define PD_ERR_CUDA 3        /* a CUDA runtime call failed                      */
+#define PD_ERR_WORKSPACE 4   /* workspace smaller than the queried size         */
+
+#define PD_METHOD_MPPCA 0   /* MPPCADenoiser      (space_time/lowrank.py:28-63)   */
+#define PD_METHOD_HYBRID 1  /* HybridPCADenoiser  (space_time/lowrank.py:67-119)  */
+#define PD_METHOD_RAW 2     /* RawSVDDenoiser / NordicDenoiser hard threshold
+                               (space_time/lowrank.py:123-246)                    */
+#define PD_METHOD_OPTIMAL 3 /* OptimalSVDDenoiser (space_time/lowrank.py:284-407) */
+
+#define PD_RECOMB_WEIGHTED 0 /* theta = 1 / (2 + maxidx)  (base.py:246-249) */
+#define PD_RECOMB_AVERAGE 1  /* theta = 1                 (base.py:250-252) */
+#define PD_RECOMB_CENTER 2   /* centre element only       (base.py:244-245) */
+
+#define PD_LOSS_FRO 0 /* _opt_fro_shrink (space_time/lowrank.py:272-280) */
+#define PD_LOSS_NUC 1 /* _opt_nuc_shrink (space_time/lowrank.py:263-269) */
+#define PD_LOSS_OPE 2 /* _opt_ope_shrink (space_time/lowrank.py:258-260) */
+
+#define PD_PRECISION_FP32 0  /* FP32 SIMT Gram                                  */
+#define PD_PRECISION_MIXED 1 /* BF16 tcgen05 Gram + FP32 subspace refinement    */
+
+/* Patch geometry of the strided sliding view.
+ * Mirrors PatchedArray.__init__ (space_time/base.py:24-82). */
+typedef struct pd_geometry {
+  int64_t shape[4]; /* (X, Y, Z, T), leading axes padded with 1            */
+  int64_t patch[4]; /* patch extent per axis (clamped to the axis)         */
+  int64_t step[4];  /* patch - overlap, taken before clamping              */
+  int64_t grid[4];  /* number of patch positions per axis                  */
+  int64_t n_patches;
+  int64_t rows; /* M = voxels per patch (Casorati rows)                    */
+  int64_t cols; /* frames per patch (Casorati columns)                     */
+} pd_geometry;
+
+/* Per-call method parameters. */
+typedef struct pd_params {
+  int32_t method;        /* PD_METHOD_*                                     */
+  int32_t recombination; /* PD_RECOMB_*                                     */
+  int32_t loss;          /* PD_LOSS_* (optimal only)                        */
+  int32_t precision;     /* PD_PRECISION_*                                  */
+  int32_t is_complex;    /* input/output are complex64                      */
+  int32_t has_prior;     /* noise_std map given (hybrid / optimal)          */
+  double threshold_scale; /* MP-PCA threshold_scale                         */
+  double threshold;       /* raw / NORDIC singular-value threshold          */
+  double mp_median;       /* optimal: Marchenko-Pastur median for beta      */
+} pd_params;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int32_t pd_version(void);
+
+/* Message of the last failing call on this host thread (empty if none). */
+const char* pd_last_error(void);
+
+/* Fill *g from the full (time-appended) patch shape and overlap.
+ * Replaces PatchedArray.__init__ (space_time/base.py:24-82) applied to the
+ * output of BaseSpaceTimeDenoiser._get_patch_param (base.py:359-384).
+ * ndim in [2, 4]; returns PD_ERR_INVALID where the reference raises. */
+pd_status pd_geometry_init(int32_t ndim, const int64_t* shape, const int64_t* patch_shape,
+                           const int64_t* patch_overlap, pd_geometry* g);
+
+/* Median of the Marchenko-Pastur law of aspect ratio beta, by the reference's
+ * 5-point dichotomy on the closed-form CDF (host, FP64).
+ * Replaces marchenko_pastur_median (space_time/utils.py:149-204). */
+pd_status pd_mp_median(double beta, double eps, double* out);
+
+/* Scratch bytes pd_select_patches needs. */
+pd_status pd_select_workspace_size(const pd_geometry* g, size_t* bytes);
+
+/* Mask scoring and compaction: d_patch_list[0 .. *d_count) receives, in
+ * ascending order, every linear patch index whose mask fill satisfies
+ * 100 * sum(mask in patch) / patch size > mask_threshold. d_mask is uint8 of
+ * shape (X,Y,Z) (mask_is_4d = 0) or (X,Y,Z,T) (mask_is_4d = 1), or NULL for an
+ * all-true mask. d_patch_list holds n_patches int32.
+ * Replaces the selection loop of BaseSpaceTimeDenoiser.denoise (base.py:202-227). */
+pd_status pd_select_patches(const pd_geometry* g, const uint8_t* d_mask, int32_t mask_is_4d,
+                            double mask_threshold, int32_t* d_patch_list, int32_t* d_count,
+                            void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* Scratch bytes pd_denoise_patches needs for n_selected patches. */
+pd_status pd_denoise_workspace_size(const pd_geometry* g, const pd_params* p, int64_t n_selected,
+                                    size_t* bytes);
+
+/* Denoise the listed patches and accumulate them.
+ *   d_in          input volume (float32 or complex64), read only
+ *   d_noise_std   spatial noise_std map (float64, X*Y*Z) when p->has_prior, else NULL
+ *   d_out_acc     output volume, same type as d_in, zeroed by the caller; receives
+ *                 sum theta * patch (weighted/average) or the centre elements
+ *   d_weight_acc  float32 [X*Y*Z*grid[3]]: sum of theta per voxel and time window
+ *   d_noise_acc   float32 [X*Y*Z*grid[3]]: sum of theta * noise_var (finite only)
+ *   d_noise_ctr   float32 4D map: centre-element noise_var (center recombination)
+ *   d_rank_map    int32 4D map: max maxidx of the patches centred on each voxel
+ *   d_patch_rank  int32 [n_selected]: maxidx per listed patch
+ *   d_patch_noise float32 [n_selected]: noise_var per listed patch (NaN if none)
+ * All accumulators are zeroed by the caller.
+ * Replaces the hot loop of BaseSpaceTimeDenoiser.denoise (base.py:235-258) and the
+ * _patch_processing plug-ins of MPPCADenoiser, HybridPCADenoiser, RawSVDDenoiser,
+ * NordicDenoiser and OptimalSVDDenoiser (space_time/lowrank.py:42-407). */
+pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const void* d_in,
+                             const double* d_noise_std, const int32_t* d_patch_list,
+                             int64_t n_selected, void* d_out_acc, float* d_weight_acc,
+                             float* d_noise_acc, float* d_noise_ctr, int32_t* d_rank_map,
+                             int32_t* d_patch_rank, float* d_patch_noise, void* d_workspace,
+                             size_t workspace_bytes, void* stream);
+
+/* Normalisation and masking: d_out /= weights (weighted/average), expand the
+ * window accumulators into the 4D float32 d_weights and d_noise_map, then zero
+ * every element outside the mask (NULL mask = all true).
+ * Replaces base.py:262-270. */
+pd_status pd_finalize(const pd_geometry* g, const pd_params* p, void* d_out,
+                      const float* d_weight_acc, const float* d_noise_acc,
+                      const float* d_noise_ctr, float* d_weights, float* d_noise_map,
+                      const uint8_t* d_mask, int32_t mask_is_4d, void* stream);
+
+/* Scratch bytes pd_nordic_mc_threshold needs. */
+pd_status pd_nordic_workspace_size(int64_t rows, int64_t cols, int32_t n_iter, size_t* bytes);
+
+/* NORDIC Monte-Carlo level: mean over n_iter draws of the largest singular value
+ * of a rows x cols standard Gaussian matrix (counter-based Philox normals, seeded),
+ * written to *out on the host. Synchronises the stream.
+ * Replaces the Monte-Carlo loop of NordicDenoiser.denoise (space_time/lowrank.py:221-232). */
+pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uint64_t seed,
+                                 int32_t precision, double* out, void* d_workspace,
+                                 size_t workspace_bytes, void* stream);
+
+/* Kernel timing (no reference counterpart; used by bench.py for the roofline).
+ * When enabled, every kernel launch of the library on this host thread's calls
+ * is bracketed by CUDA events on its stream. pd_profile_collect synchronises
+ * those events and writes one line per kernel, "name launches total_ms\n", into
+ * buf (truncated to len), then clears the record. */
+pd_status pd_profile_enable(int32_t on);
+pd_status pd_profile_collect(char* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PATCH_DENOISE_B200_H */

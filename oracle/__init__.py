@@ -1,0 +1,20 @@
+"""CPU oracle for the space-time low-rank denoising path. TEST INFRASTRUCTURE ONLY.
+
+Nothing in the product package imports this. Only ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use it, and only
+as the checker / the timed CPU reference arm.
+"""
+
+from .oracle import (  # noqa: F401
+    METHODS,
+    denoise,
+    eig_analysis,
+    eig_synthesis,
+    grid_geometry,
+    marchenko_pastur_median,
+    nordic_threshold,
+    patch_params,
+    select_patches,
+    svd_analysis,
+    svd_synthesis,
+)

@@ -1,0 +1,180 @@
+"""Device orchestration of one ``denoise()`` call through the C ABI.
+
+PyTorch provides device memory and the stream; every computation on the volume
+runs in ``libpd_b200.so``. The call sequence mirrors
+``BaseSpaceTimeDenoiser.denoise`` (space_time/base.py:177-270):
+
+  pd_select_patches   mask scoring + ascending list of kept patches (base.py:202-227)
+  pd_denoise_patches  per-patch decomposition, threshold, synthesis, scatter (base.py:235-258)
+  pd_finalize         normalisation by the weights, masking (base.py:262-270)
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def _vp(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def geometry(shape, p_s, p_o) -> _lib.Geometry:
+    """``pd_geometry_init`` over the full (time-appended) patch shape and overlap."""
+    lib = _lib.load()
+    nd = len(shape)
+    arr = lambda v: (ctypes.c_int64 * nd)(*[int(x) for x in v])  # noqa: E731
+    g = _lib.Geometry()
+    _lib.check(lib.pd_geometry_init(nd, arr(shape), arr(p_s), arr(p_o), ctypes.byref(g)))
+    return g
+
+
+def mp_median(beta: float, eps: float = 1e-7) -> float:
+    """Marchenko-Pastur median (``pd_mp_median``)."""
+    out = ctypes.c_double()
+    _lib.check(_lib.load().pd_mp_median(float(beta), float(eps), ctypes.byref(out)))
+    return out.value
+
+
+def nordic_max_sval(rows: int, cols: int, n_iter: int, seed: int, device, precision: str = "fp32") -> float:
+    """Mean largest singular value of ``n_iter`` Gaussian rows x cols draws."""
+    lib = _lib.load()
+    need = ctypes.c_size_t()
+    _lib.check(lib.pd_nordic_workspace_size(int(rows), int(cols), int(n_iter), ctypes.byref(need)))
+    ws = torch.empty(max(need.value, 1), dtype=torch.uint8, device=device)
+    out = ctypes.c_double()
+    _lib.check(
+        lib.pd_nordic_mc_threshold(
+            int(rows), int(cols), int(n_iter), ctypes.c_uint64(int(seed) & (2**64 - 1)),
+            _lib.PRECISION[precision], ctypes.byref(out), _vp(ws), need.value, _stream(device),
+        )
+    )
+    return out.value
+
+
+@dataclass
+class DeviceResult:
+    """Outputs of one call, on the device."""
+
+    out: torch.Tensor
+    weights: torch.Tensor
+    noise_map: torch.Tensor
+    rank_map: torch.Tensor
+    patch_index: torch.Tensor
+    patch_rank: torch.Tensor
+    patch_noise: torch.Tensor
+
+
+def compute_dtype(dtype) -> torch.dtype:
+    """Arithmetic type of the CUDA path for an input dtype."""
+    if dtype in (torch.complex64, torch.complex128, np.complex64, np.complex128):
+        return torch.complex64
+    return torch.float32
+
+
+def to_device(x, device, dtype=None, pin=False) -> torch.Tensor:
+    if isinstance(x, torch.Tensor):
+        t = x
+    else:
+        a = np.ascontiguousarray(x)
+        t = torch.from_numpy(a)
+        if pin:
+            t = t.pin_memory()
+    if dtype is not None and t.dtype != dtype:
+        t = t.to(dtype)
+    return t.to(device, non_blocking=pin).contiguous()
+
+
+def run(
+    method: str,
+    data: torch.Tensor,
+    p_s,
+    p_o,
+    recombination: str,
+    mask: torch.Tensor | None,
+    mask_threshold: float,
+    *,
+    threshold_scale: float = 1.0,
+    threshold: float = 0.0,
+    noise_std: torch.Tensor | None = None,
+    loss: str = "fro",
+    mp_med: float = 0.0,
+    precision: str = "fp32",
+) -> DeviceResult:
+    """Denoise ``data`` (device tensor, float32 or complex64, C-contiguous).
+
+    ``mask``: uint8 device tensor of the data shape or of its spatial shape, or None.
+    ``noise_std``: float64 device tensor of the spatial shape, or None.
+    """
+    lib = _lib.load()
+    device = data.device
+    if device.type != "cuda":
+        raise RuntimeError("the denoising path runs on a CUDA device only")
+    cplx = data.is_complex()
+    shape = tuple(data.shape)
+    g = geometry(shape, p_s, p_o)
+    s = _stream(device)
+    gp = ctypes.byref(g)
+
+    # ---- selection
+    need = ctypes.c_size_t()
+    _lib.check(lib.pd_select_workspace_size(gp, ctypes.byref(need)))
+    ws = torch.empty(max(need.value, 1), dtype=torch.uint8, device=device)
+    plist = torch.empty(max(g.n_patches, 1), dtype=torch.int32, device=device)
+    count = torch.zeros(1, dtype=torch.int32, device=device)
+    mask_4d = 0
+    if mask is not None:
+        mask_4d = 1 if mask.dim() == len(shape) else 0
+    _lib.check(
+        lib.pd_select_patches(gp, _vp(mask), mask_4d, float(mask_threshold), _vp(plist), _vp(count), _vp(ws),
+                              need.value, s)
+    )
+    n_sel = int(count.item())
+
+    # ---- parameters
+    prm = _lib.Params()
+    prm.method = _lib.METHOD[method]
+    prm.recombination = _lib.RECOMBINATION[recombination]
+    prm.loss = _lib.LOSS[loss]
+    prm.precision = _lib.PRECISION[precision]
+    prm.is_complex = 1 if cplx else 0
+    prm.has_prior = 1 if noise_std is not None else 0
+    prm.threshold_scale = float(threshold_scale)
+    prm.threshold = float(threshold)
+    prm.mp_median = float(mp_med)
+    pp = ctypes.byref(prm)
+
+    # ---- accumulators and outputs
+    full = (int(g.shape[0]), int(g.shape[1]), int(g.shape[2]), int(g.shape[3]))
+    nvox = full[0] * full[1] * full[2]
+    out = torch.zeros(shape, dtype=data.dtype, device=device)
+    wacc = torch.zeros(nvox * int(g.grid[3]), dtype=torch.float32, device=device)
+    nacc = torch.zeros_like(wacc)
+    nctr = torch.zeros(shape, dtype=torch.float32, device=device)
+    rank_map = torch.zeros(shape, dtype=torch.int32, device=device)
+    prank = torch.zeros(max(n_sel, 1), dtype=torch.int32, device=device)
+    pnoise = torch.zeros(max(n_sel, 1), dtype=torch.float32, device=device)
+    _lib.check(lib.pd_denoise_workspace_size(gp, pp, n_sel, ctypes.byref(need)))
+    ws = torch.empty(max(need.value, 1), dtype=torch.uint8, device=device)
+    _lib.check(
+        lib.pd_denoise_patches(
+            gp, pp, _vp(data), _vp(noise_std), _vp(plist), n_sel, _vp(out), _vp(wacc), _vp(nacc), _vp(nctr),
+            _vp(rank_map), _vp(prank), _vp(pnoise), _vp(ws), need.value, s,
+        )
+    )
+    weights = torch.empty(shape, dtype=torch.float32, device=device)
+    noise_map = torch.empty(shape, dtype=torch.float32, device=device)
+    _lib.check(
+        lib.pd_finalize(gp, pp, _vp(out), _vp(wacc), _vp(nacc), _vp(nctr), _vp(weights), _vp(noise_map), _vp(mask),
+                        mask_4d, s)
+    )
+    return DeviceResult(out, weights, noise_map, rank_map, plist[:n_sel], prank[:n_sel], pnoise[:n_sel])

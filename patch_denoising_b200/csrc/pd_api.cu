@@ -1,0 +1,429 @@
+// C ABI of libpd_b200.so: argument checking, workspace carving and the launch
+// sequence. See include/patch_denoise_b200.h for the contract of each call.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <string>
+
+#include "pd_common.cuh"
+#include "pd_kernels.cuh"
+#include "pd_profile.cuh"
+
+using namespace pd;
+
+namespace {
+
+thread_local std::string g_err;
+
+pd_status fail(pd_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return st;
+}
+
+pd_status cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) return fail(PD_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return PD_OK;
+}
+
+#define PD_TRY(x)                      \
+  do {                                 \
+    const pd_status _st = (x);         \
+    if (_st != PD_OK) return _st;      \
+  } while (0)
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Carver {
+  char* base;
+  size_t off = 0;
+  explicit Carver(void* b) : base((char*)b) {}
+  template <class T>
+  T* take(size_t count) {
+    T* p = (T*)(base ? base + off : nullptr);
+    off += align256(count * sizeof(T));
+    return p;
+  }
+};
+
+constexpr int MAX_FRAMES = 448;
+constexpr int MAX_ROWS = 16384;
+constexpr size_t DEFAULT_CHUNK_BUDGET = size_t(4) << 30;
+
+int64_t gram_stride_floats(int n, bool cplx) {
+  int64_t f = pk_size(n) * (cplx ? 2 : 1);
+  return (f + 63) & ~int64_t(63);
+}
+int64_t vec_stride_floats(int n) { return ((int64_t)2 * n * n + 63) & ~int64_t(63); }
+
+size_t per_patch_bytes(int n, bool cplx) {
+  Carver c(nullptr);
+  // carve one patch worth of every buffer (upper bound incl. alignment)
+  size_t b = 0;
+  b += (size_t)n * (cplx ? 8 : 4);                  // mean
+  b += (size_t)gram_stride_floats(n, cplx) * 4;     // gram
+  b += (size_t)vec_stride_floats(n) * 4;            // vec
+  b += (size_t)n * 4;                               // coef
+  b += 4 + 4 + 4 + 8;                               // n_active, rank, noise, prior
+  (void)c;
+  return b;
+}
+
+PatchWork carve_work(void* ws, int count, int n, bool cplx, size_t* used) {
+  Carver c(ws);
+  PatchWork w{};
+  w.count = count;
+  w.mean = c.take<float>((size_t)count * n * (cplx ? 2 : 1));
+  w.gram_stride = gram_stride_floats(n, cplx);
+  w.gram = c.take<float>((size_t)count * w.gram_stride);
+  w.vec_stride = vec_stride_floats(n);
+  w.vec = c.take<float>((size_t)count * w.vec_stride);
+  w.coef = c.take<float>((size_t)count * n);
+  w.n_active = c.take<int32_t>(count);
+  w.rank = c.take<int32_t>(count);
+  w.noise = c.take<float>(count);
+  w.prior = c.take<double>(count);
+  *used = c.off;
+  return w;
+}
+
+size_t work_bytes(int count, int n, bool cplx) {
+  size_t used;
+  carve_work(nullptr, count, n, cplx, &used);
+  return used;
+}
+
+pd_status check_geometry(const pd_geometry* g) {
+  if (!g) return fail(PD_ERR_INVALID, "geometry is NULL");
+  for (int i = 0; i < 4; ++i)
+    if (g->shape[i] < 1 || g->patch[i] < 1 || g->grid[i] < 1)
+      return fail(PD_ERR_INVALID, "geometry is not initialised");
+  return PD_OK;
+}
+
+pd_status check_params(const pd_geometry* g, const pd_params* p) {
+  if (!p) return fail(PD_ERR_INVALID, "params is NULL");
+  if (p->method < PD_METHOD_MPPCA || p->method > PD_METHOD_OPTIMAL)
+    return fail(PD_ERR_INVALID, "unknown method %d", p->method);
+  if (p->recombination < PD_RECOMB_WEIGHTED || p->recombination > PD_RECOMB_CENTER)
+    return fail(PD_ERR_INVALID, "recombination must be one of 'weighted', 'average', 'center'");
+  if (p->loss < PD_LOSS_FRO || p->loss > PD_LOSS_OPE) return fail(PD_ERR_INVALID, "unknown loss %d", p->loss);
+  const int64_t n = g->cols, M = g->rows;
+  if (n > MAX_FRAMES)
+    return fail(PD_ERR_UNSUPPORTED, "patch spans %lld frames; this build handles at most %d", (long long)n,
+                MAX_FRAMES);
+  if (M > MAX_ROWS)
+    return fail(PD_ERR_UNSUPPORTED, "patch has %lld voxels; this build handles at most %d", (long long)M,
+                MAX_ROWS);
+  if (M < 2) return fail(PD_ERR_INVALID, "a patch needs at least 2 voxels");
+  if ((p->method == PD_METHOD_MPPCA || p->method == PD_METHOD_HYBRID) && n < 10)
+    return fail(PD_ERR_INVALID, "MP-PCA / hybrid-PCA need at least 10 frames per patch (top-10 eigenvalues)");
+  if (p->precision != PD_PRECISION_FP32 && p->precision != PD_PRECISION_MIXED)
+    return fail(PD_ERR_INVALID, "unknown precision %d", p->precision);
+  return PD_OK;
+}
+
+// Marchenko-Pastur CDF, closed form of the integral of
+// sqrt((b-t)(t-a)) / (2 pi beta t) from a to x, a = (1-sqrt(beta))^2, b = (1+sqrt(beta))^2.
+// Antiderivative: R + (a+b)/2 asin((2t-a-b)/(b-a)) - sqrt(ab) asin(((a+b)t-2ab)/((b-a)t)).
+double mp_cdf(double x, double beta) {
+  const double a = (1 - sqrt(beta)) * (1 - sqrt(beta));
+  const double b = (1 + sqrt(beta)) * (1 + sqrt(beta));
+  if (x <= a) return 0.0;
+  if (x >= b) return 1.0;
+  auto clamp1 = [](double u) { return u > 1.0 ? 1.0 : (u < -1.0 ? -1.0 : u); };
+  auto G = [&](double t) {
+    const double R = sqrt(fmax((b - t) * (t - a), 0.0));
+    double v = R + 0.5 * (a + b) * asin(clamp1((2 * t - a - b) / (b - a)));
+    const double sab = sqrt(a * b);
+    if (sab > 0.0) v -= sab * asin(clamp1(((a + b) * t - 2 * a * b) / ((b - a) * t)));
+    return v;
+  };
+  return (G(x) - G(a)) / (2.0 * M_PI * beta);
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t pd_version(void) { return 100; }
+
+const char* pd_last_error(void) { return g_err.c_str(); }
+
+pd_status pd_geometry_init(int32_t ndim, const int64_t* shape, const int64_t* patch_shape,
+                           const int64_t* patch_overlap, pd_geometry* g) {
+  g_err.clear();
+  if (!shape || !patch_shape || !patch_overlap || !g) return fail(PD_ERR_INVALID, "NULL argument");
+  if (ndim < 2 || ndim > 4)
+    return fail(PD_ERR_UNSUPPORTED, "inputs with %d dimensions are not supported (2 to 4)", ndim);
+  int64_t ps[4], st[4], sh[4], gr[4];
+  const int pad = 4 - ndim;
+  for (int i = 0; i < 4; ++i) {
+    if (i < pad) {
+      sh[i] = 1;
+      ps[i] = 1;
+      st[i] = 1;
+      gr[i] = 1;
+      continue;
+    }
+    const int k = i - pad;
+    sh[i] = shape[k];
+    if (sh[i] < 1) return fail(PD_ERR_INVALID, "empty input axis %d", k);
+    const int64_t step = patch_shape[k] - patch_overlap[k];
+    if (step < 0) return fail(PD_ERR_INVALID, "overlap should be smaller than patch on every dimension.");
+    if (patch_shape[k] < 1) return fail(PD_ERR_INVALID, "patch extent must be positive");
+    if (patch_shape[k] > sh[i])
+      return fail(PD_ERR_INVALID,
+                  "patch extent %lld exceeds the input extent %lld along axis %d (the Casorati reshape of the "
+                  "reference fails)",
+                  (long long)patch_shape[k], (long long)sh[i], k);
+    ps[i] = patch_shape[k];
+    st[i] = step;
+    if (ps[i] < sh[i])
+      gr[i] = step > 0 ? (sh[i] - ps[i]) / step + 1 : 1;
+    else
+      gr[i] = 1;
+  }
+  int64_t np = 1;
+  for (int i = 0; i < 4; ++i) {
+    g->shape[i] = sh[i];
+    g->patch[i] = ps[i];
+    g->step[i] = st[i];
+    g->grid[i] = gr[i];
+    np *= gr[i];
+  }
+  if (np > INT32_MAX) return fail(PD_ERR_UNSUPPORTED, "more than 2^31 patches");
+  g->n_patches = np;
+  g->rows = ps[0] * ps[1] * ps[2];
+  g->cols = ps[3];
+  return PD_OK;
+}
+
+pd_status pd_mp_median(double beta, double eps, double* out) {
+  g_err.clear();
+  if (!out) return fail(PD_ERR_INVALID, "NULL output");
+  if (!(0 <= beta && beta <= 1)) return fail(PD_ERR_INVALID, "Aspect Ratio should be between 0 and 1");
+  const double a = (1 - sqrt(beta)) * (1 - sqrt(beta));
+  const double b = (1 + sqrt(beta)) * (1 + sqrt(beta));
+  double lo = a, hi = b;
+  bool moved = true;
+  int rounds = 0;
+  while (moved && (hi - lo) > eps && rounds < 20) {
+    moved = false;
+    double pts[5];
+    const double step = (hi - lo) / 4.0;
+    for (int i = 0; i < 4; ++i) pts[i] = (double)i * step + lo;
+    pts[4] = hi;
+    double cdf[5];
+    for (int i = 0; i < 5; ++i) cdf[i] = mp_cdf(pts[i], beta);
+    bool any_lo = false, any_hi = false;
+    double nlo = -INFINITY, nhi = INFINITY;
+    for (int i = 0; i < 5; ++i) {
+      if (cdf[i] < 0.5) {
+        any_lo = true;
+        nlo = fmax(nlo, pts[i]);
+      }
+      if (cdf[i] > 0.5) {
+        any_hi = true;
+        nhi = fmin(nhi, pts[i]);
+      }
+    }
+    if (any_lo) {
+      lo = nlo;
+      moved = true;
+    }
+    if (any_hi) {
+      hi = nhi;
+      moved = true;
+    }
+    ++rounds;
+  }
+  *out = (lo + hi) / 2;
+  return PD_OK;
+}
+
+pd_status pd_select_workspace_size(const pd_geometry* g, size_t* bytes) {
+  g_err.clear();
+  PD_TRY(check_geometry(g));
+  if (!bytes) return fail(PD_ERR_INVALID, "NULL output");
+  const int64_t np = g->n_patches;
+  const int64_t nb = (np + SEL_BLOCK - 1) / SEL_BLOCK;
+  const int64_t nvox = g->shape[0] * g->shape[1] * g->shape[2];
+  *bytes = align256(np) + align256(sizeof(int32_t) * nb) + align256(sizeof(int32_t) * nvox * g->grid[3]);
+  return PD_OK;
+}
+
+pd_status pd_select_patches(const pd_geometry* g, const uint8_t* d_mask, int32_t mask_is_4d, double mask_threshold,
+                            int32_t* d_patch_list, int32_t* d_count, void* d_ws, size_t ws_bytes, void* stream) {
+  g_err.clear();
+  PD_TRY(check_geometry(g));
+  if (!d_patch_list || !d_count) return fail(PD_ERR_INVALID, "NULL output buffer");
+  size_t need;
+  PD_TRY(pd_select_workspace_size(g, &need));
+  if (ws_bytes < need || !d_ws) return fail(PD_ERR_WORKSPACE, "select workspace too small (%zu < %zu)", ws_bytes, need);
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geo G = to_geo(*g);
+  const int64_t np = g->n_patches;
+  const int64_t nb = (np + SEL_BLOCK - 1) / SEL_BLOCK;
+  Carver c(d_ws);
+  uint8_t* flags = c.take<uint8_t>(np);
+  int32_t* bc = c.take<int32_t>(nb);
+  int32_t* cnt = c.take<int32_t>(g->shape[0] * g->shape[1] * g->shape[2] * g->grid[3]);
+  int mode = 0;
+  if (d_mask) {
+    if (mask_is_4d) {
+      mode = 2;
+      const int64_t tot = g->shape[0] * g->shape[1] * g->shape[2] * g->grid[3];
+      const int blocks = (int)std::min<int64_t>((tot + 255) / 256, 148 * 16);
+      PD_TIMED("select", s, k_window_counts<<<blocks, 256, 0, s>>>(G, d_mask, cnt));
+    } else {
+      mode = 1;
+    }
+  }
+  {
+    const int64_t warps = np;
+    const int blocks = (int)std::min<int64_t>((warps * 32 + 255) / 256, 148 * 64);
+    PD_TIMED("select", s,
+             k_patch_flags<<<blocks, 256, 0, s>>>(G, mode, mode == 1 ? d_mask : nullptr, cnt, mask_threshold, flags));
+  }
+  PD_TIMED("select", s, k_block_counts<<<(unsigned)nb, SEL_THREADS, 0, s>>>(flags, np, bc));
+  PD_TIMED("select", s, k_scan_counts<<<1, 1024, 0, s>>>(bc, nb, d_count));
+  PD_TIMED("select", s, k_compact<<<(unsigned)nb, SEL_THREADS, 0, s>>>(flags, np, bc, d_patch_list));
+  return cuda_check(cudaGetLastError(), "pd_select_patches launch");
+}
+
+pd_status pd_denoise_workspace_size(const pd_geometry* g, const pd_params* p, int64_t n_selected, size_t* bytes) {
+  g_err.clear();
+  PD_TRY(check_geometry(g));
+  PD_TRY(check_params(g, p));
+  if (!bytes) return fail(PD_ERR_INVALID, "NULL output");
+  if (n_selected < 0) return fail(PD_ERR_INVALID, "negative patch count");
+  const int n = (int)g->cols;
+  const bool cplx = p->is_complex != 0;
+  const size_t pp = per_patch_bytes(n, cplx);
+  int64_t chunk = (int64_t)std::max<size_t>(1, DEFAULT_CHUNK_BUDGET / pp);
+  chunk = std::min<int64_t>(chunk, std::max<int64_t>(n_selected, 1));
+  *bytes = work_bytes((int)chunk, n, cplx);
+  return PD_OK;
+}
+
+pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const void* d_in, const double* d_noise_std,
+                             const int32_t* d_patch_list, int64_t n_selected, void* d_out_acc, float* d_weight_acc,
+                             float* d_noise_acc, float* d_noise_ctr, int32_t* d_rank_map, int32_t* d_patch_rank,
+                             float* d_patch_noise, void* d_ws, size_t ws_bytes, void* stream) {
+  g_err.clear();
+  PD_TRY(check_geometry(g));
+  PD_TRY(check_params(g, p));
+  if (n_selected == 0) return PD_OK;
+  if (!d_in || !d_patch_list || !d_out_acc || !d_weight_acc || !d_noise_acc || !d_noise_ctr || !d_rank_map ||
+      !d_patch_rank || !d_patch_noise)
+    return fail(PD_ERR_INVALID, "NULL buffer");
+  if ((p->method == PD_METHOD_HYBRID || (p->method == PD_METHOD_OPTIMAL && p->has_prior)) && !d_noise_std)
+    return fail(PD_ERR_INVALID, "this method needs the noise_std map");
+  if (p->precision == PD_PRECISION_MIXED)
+    return fail(PD_ERR_UNSUPPORTED, "mixed precision is not built in this library");
+  const int n = (int)g->cols;
+  const bool cplx = p->is_complex != 0;
+  const size_t one = work_bytes(1, n, cplx);
+  if (!d_ws || ws_bytes < one) return fail(PD_ERR_WORKSPACE, "workspace too small (%zu < %zu)", ws_bytes, one);
+  // largest chunk that fits
+  int64_t chunk = std::max<int64_t>(1, (int64_t)(ws_bytes / per_patch_bytes(n, cplx)));
+  chunk = std::min<int64_t>(chunk, n_selected);
+  while (chunk > 1 && work_bytes((int)chunk, n, cplx) > ws_bytes) --chunk;
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geo G = to_geo(*g);
+  EigParams ep;
+  ep.method = p->method;
+  ep.loss = p->loss;
+  ep.has_prior = p->has_prior;
+  ep.rows = (int)g->rows;
+  ep.cols = n;
+  ep.threshold_scale = p->threshold_scale;
+  ep.threshold = p->threshold;
+  ep.mp_median = p->mp_median;
+  for (int64_t off = 0; off < n_selected; off += chunk) {
+    const int cnt = (int)std::min<int64_t>(chunk, n_selected - off);
+    size_t used;
+    PatchWork w = carve_work(d_ws, cnt, n, cplx, &used);
+    w.list = d_patch_list + off;
+    launch_patch_mean(G, cplx, d_in, w, s);
+    if (p->method == PD_METHOD_HYBRID || (p->method == PD_METHOD_OPTIMAL && p->has_prior))
+      launch_prior(G, p->method, d_noise_std, w, s);
+    launch_gram_fp32(G, cplx, d_in, w, s);
+    PD_TRY(cuda_check(launch_eig(cplx, n, ep, w, s), "eigensolver launch"));
+    SynthArgs sa;
+    sa.recombination = p->recombination;
+    sa.out = d_out_acc;
+    sa.weight_acc = d_weight_acc;
+    sa.noise_acc = d_noise_acc;
+    sa.noise_ctr = d_noise_ctr;
+    sa.rank_map = d_rank_map;
+    sa.patch_rank = d_patch_rank;
+    sa.patch_noise = d_patch_noise;
+    sa.list_offset = off;
+    launch_synth(G, cplx, d_in, w, sa, s);
+    PD_TRY(cuda_check(cudaGetLastError(), "pd_denoise_patches launch"));
+  }
+  return PD_OK;
+}
+
+pd_status pd_finalize(const pd_geometry* g, const pd_params* p, void* d_out, const float* d_weight_acc,
+                      const float* d_noise_acc, const float* d_noise_ctr, float* d_weights, float* d_noise_map,
+                      const uint8_t* d_mask, int32_t mask_is_4d, void* stream) {
+  g_err.clear();
+  PD_TRY(check_geometry(g));
+  if (!p) return fail(PD_ERR_INVALID, "params is NULL");
+  if (!d_out || !d_weight_acc || !d_noise_acc || !d_noise_ctr || !d_weights || !d_noise_map)
+    return fail(PD_ERR_INVALID, "NULL buffer");
+  launch_finalize(to_geo(*g), p->is_complex != 0, p->recombination, d_out, d_weight_acc, d_noise_acc, d_noise_ctr,
+                  d_weights, d_noise_map, d_mask, mask_is_4d, (cudaStream_t)stream);
+  return cuda_check(cudaGetLastError(), "pd_finalize launch");
+}
+
+pd_status pd_nordic_workspace_size(int64_t rows, int64_t cols, int32_t n_iter, size_t* bytes) {
+  g_err.clear();
+  if (!bytes) return fail(PD_ERR_INVALID, "NULL output");
+  if (rows < 1 || cols < 1 || n_iter < 1) return fail(PD_ERR_INVALID, "empty Monte-Carlo problem");
+  if (cols > MAX_FRAMES) return fail(PD_ERR_UNSUPPORTED, "at most %d frames", MAX_FRAMES);
+  *bytes = work_bytes(n_iter, (int)cols, false) +
+           align256(sizeof(float) * (size_t)n_iter * mc_chunks(rows) * pk_size((int)cols));
+  return PD_OK;
+}
+
+pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uint64_t seed, int32_t precision,
+                                 double* out, void* d_ws, size_t ws_bytes, void* stream) {
+  g_err.clear();
+  if (!out) return fail(PD_ERR_INVALID, "NULL output");
+  size_t need;
+  PD_TRY(pd_nordic_workspace_size(rows, cols, n_iter, &need));
+  if (!d_ws || ws_bytes < need) return fail(PD_ERR_WORKSPACE, "workspace too small (%zu < %zu)", ws_bytes, need);
+  (void)precision;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n = (int)cols;
+  size_t used;
+  PatchWork w = carve_work(d_ws, n_iter, n, false, &used);
+  float* part = (float*)((char*)d_ws + used);
+  launch_mc_gram(rows, n, n_iter, seed, part, w.gram, w.gram_stride, s);
+  EigParams ep{};
+  ep.method = EIG_MODE_TOP1;
+  ep.rows = (int)std::min<int64_t>(rows, INT32_MAX);
+  ep.cols = n;
+  PD_TRY(cuda_check(launch_eig(false, n, ep, w, s), "Monte-Carlo eigensolver launch"));
+  double lam[4096];
+  if (n_iter > 4096) return fail(PD_ERR_UNSUPPORTED, "at most 4096 Monte-Carlo draws");
+  PD_TRY(cuda_check(cudaMemcpyAsync(lam, w.prior, sizeof(double) * n_iter, cudaMemcpyDeviceToHost, s), "copy"));
+  PD_TRY(cuda_check(cudaStreamSynchronize(s), "Monte-Carlo sync"));
+  double acc = 0.0;
+  for (int i = 0; i < n_iter; ++i) acc += sqrt(fmax(lam[i], 0.0));
+  *out = acc / n_iter;
+  return PD_OK;
+}
+
+}  // extern "C"

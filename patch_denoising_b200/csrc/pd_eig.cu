@@ -1,0 +1,716 @@
+// Per-patch Hermitian eigensolver and threshold rules (one CTA per patch).
+//
+//  1. The packed lower Gram C = Xc^H Xc (n = frames) is staged in shared memory
+//     when it fits (else worked on in place in global memory) and scaled by
+//     1 / max(diag).
+//  2. Householder reduction to real symmetric tridiagonal form T = Q^H C Q
+//     (H_j = I - tau_j v_j v_j^H, v_j stored below the subdiagonal), the
+//     classical unblocked algorithm (Golub & Van Loan, sec. 8.3.1).
+//  3. Eigenvalues of T at requested indices by Sturm-count multisection: one
+//     warp evaluates 32 points per round, shrinking the bracket 33x.
+//  4. The reference threshold rule of the method, evaluated in FP64 on the
+//     eigenvalues (space_time/lowrank.py: MP-PCA :42-63, Hybrid :104-119,
+//     Raw/NORDIC :170-184, Optimal :379-407), gives maxidx, noise_var and the
+//     active components with their synthesis coefficients.
+//  5. Eigenvectors of T for the active components by the twisted factorisation
+//     (Parlett & Dhillon, 1997), re-orthogonalised inside eigenvalue clusters,
+//     then back-transformed by the reflectors: eigenvectors of C.
+#include <float.h>
+
+#include "pd_common.cuh"
+#include "pd_kernels.cuh"
+#include "pd_profile.cuh"
+
+namespace pd {
+
+constexpr int EIG_THREADS = 256;
+constexpr int EIG_NW = EIG_THREADS / 32;
+constexpr int MAX_SLOTS = 14;  // n <= 448
+constexpr float CAND_MARGIN = 1e-3f;
+
+struct EigLayout {
+  size_t a, d, e, e2, tau, vb, wb, idx, lam, aidx, alam, acoef, total;
+};
+
+__host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
+
+__host__ __device__ inline EigLayout eig_layout(bool cplx, int n, bool in_smem) {
+  const size_t es = cplx ? 8 : 4;
+  EigLayout L;
+  size_t o = 0;
+  L.a = o;
+  o += in_smem ? al16((size_t)pk_size(n) * es) : 0;
+  L.d = o;
+  o += al16(4 * (size_t)n);
+  L.e = o;
+  o += al16(4 * (size_t)n);
+  L.e2 = o;
+  o += al16(4 * (size_t)n);
+  L.tau = o;
+  o += al16(es * n);
+  L.vb = o;
+  o += al16(es * n);
+  L.wb = o;
+  o += al16(es * n);
+  L.idx = o;
+  o += al16(4 * (size_t)n);
+  L.lam = o;
+  o += al16(4 * (size_t)n);
+  L.aidx = o;
+  o += al16(4 * (size_t)n);
+  L.alam = o;
+  o += al16(4 * (size_t)n);
+  L.acoef = o;
+  o += al16(4 * (size_t)n);
+  L.total = o;
+  return L;
+}
+
+constexpr size_t EIG_SMEM_LIMIT = 227 * 1024 - 2048;  // leave room for static shared
+
+size_t eig_smem_bytes(bool cplx, int n, bool* in_smem) {
+  EigLayout L = eig_layout(cplx, n, true);
+  if (L.total <= EIG_SMEM_LIMIT) {
+    *in_smem = true;
+    return L.total;
+  }
+  *in_smem = false;
+  return eig_layout(cplx, n, false).total;
+}
+
+// ---------------------------------------------------------------------------
+// Reductions with static shared scratch
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float bsum_f(float v) {
+  __shared__ float red[32];
+  return block_sum<float>(v, red);
+}
+__device__ __forceinline__ cf bsum_c(cf v) {
+  __shared__ cf redc[32];
+  return block_sum<cf>(v, redc);
+}
+template <class T>
+__device__ __forceinline__ T bsum(T v);
+template <>
+__device__ __forceinline__ float bsum<float>(float v) { return bsum_f(v); }
+template <>
+__device__ __forceinline__ cf bsum<cf>(cf v) { return bsum_c(v); }
+
+__device__ __forceinline__ float bmax_f(float v) {
+  __shared__ float red[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  float r = lane < EIG_NW ? red[lane] : -FLT_MAX;
+  return warp_max(r);
+}
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Householder tridiagonalisation (lower storage, packed)
+// ---------------------------------------------------------------------------
+template <bool CPLX>
+__device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float* e,
+                               typename Elem<CPLX>::T* tau, typename Elem<CPLX>::T* vb,
+                               typename Elem<CPLX>::T* wb) {
+  using T = typename Elem<CPLX>::T;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  __shared__ T s_tau, s_inv;
+  for (int j = 0; j < n - 1; ++j) {
+    const int m = n - j - 1;
+    if (tid == 0) d[j] = re(A[pk(j, j, n)]);
+    // squared norm of the column below the subdiagonal element
+    float part = 0.f;
+    for (int i = j + 2 + tid; i < n; i += EIG_THREADS) part += abs2(A[pk(i, j, n)]);
+    const float xn2 = bsum_f(part);
+    if (tid == 0) {
+      const T alpha = A[pk(j + 1, j, n)];
+      const float ar = re(alpha);
+      float ai = 0.f;
+      if constexpr (CPLX) ai = alpha.y;
+      if (xn2 == 0.f && ai == 0.f) {
+        s_tau = zero<T>();
+        e[j] = ar;
+      } else {
+        const float nrm = sqrtf(ar * ar + ai * ai + xn2);
+        const float beta = ar >= 0.f ? -nrm : nrm;
+        if constexpr (CPLX) {
+          s_tau = cf{(beta - ar) / beta, -ai / beta};
+          // 1 / (alpha - beta)
+          const float dr = ar - beta, di = ai;
+          const float den = dr * dr + di * di;
+          s_inv = cf{dr / den, -di / den};
+        } else {
+          s_tau = (beta - ar) / beta;
+          s_inv = 1.f / (ar - beta);
+        }
+        e[j] = beta;
+      }
+      tau[j] = s_tau;
+    }
+    __syncthreads();
+    const T tj = s_tau;
+    if (re(tj) == 0.f && abs2(tj) == 0.f) continue;
+    const T inv = s_inv;
+    // v = (1, x * inv); the scaled tail is kept in A as the reflector
+    for (int i = tid; i < m; i += EIG_THREADS) {
+      T v;
+      if (i == 0) {
+        if constexpr (CPLX) v = cf{1.f, 0.f};
+        else v = 1.f;
+      } else {
+        const int64_t q = pk(j + 1 + i, j, n);
+        v = mul(A[q], inv);
+        A[q] = v;
+      }
+      vb[i] = v;
+    }
+    __syncthreads();
+    // p = A22 v, lower part (k <= i): one thread per row
+    for (int i = tid; i < m; i += EIG_THREADS) {
+      T s = zero<T>();
+      const int gi = j + 1 + i;
+      for (int k = 0; k <= i; ++k) s = s + mul(A[pk(gi, j + 1 + k, n)], vb[k]);
+      wb[i] = s;
+    }
+    __syncthreads();
+    // strictly upper part: p_k += sum_{i>k} conj(A22(i,k)) v_i, one warp per column
+    for (int k = warp; k < m; k += EIG_NW) {
+      T s = zero<T>();
+      const int64_t cb = pk(j + 1 + k, j + 1 + k, n);
+      for (int i = k + 1 + lane; i < m; i += 32) s = s + cmulc(A[cb + (i - k)], vb[i]);
+      s = warp_sum(s);
+      if (lane == 0) wb[k] = wb[k] + s;
+    }
+    __syncthreads();
+    // w = tau p ; alpha2 = -tau/2 (w^H v) ; w += alpha2 v
+    T dpart = zero<T>();
+    for (int i = tid; i < m; i += EIG_THREADS) {
+      const T wi = mul(tj, wb[i]);
+      wb[i] = wi;
+      dpart = dpart + cmulc(wi, vb[i]);
+    }
+    const T dot = bsum<T>(dpart);
+    const T a2 = mul(tj, dot) * -0.5f;
+    for (int i = tid; i < m; i += EIG_THREADS) wb[i] = wb[i] + mul(a2, vb[i]);
+    __syncthreads();
+    // A22 -= v w^H + w v^H  (lower), one warp per column
+    for (int k = warp; k < m; k += EIG_NW) {
+      const T vk = cj(vb[k]), wk = cj(wb[k]);
+      const int64_t cb = pk(j + 1 + k, j + 1 + k, n);
+      for (int i = k + lane; i < m; i += 32) {
+        const int64_t q = cb + (i - k);
+        A[q] = A[q] - (mul(vb[i], wk) + mul(wb[i], vk));
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    d[n - 1] = re(A[pk(n - 1, n - 1, n)]);
+    if (n == 1) e[0] = 0.f;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Sturm counts and multisection
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int sturm_count(const float* d, const float* e2, int n, float x, float pivmin) {
+  float q = d[0] - x;
+  if (fabsf(q) < pivmin) q = -pivmin;
+  int c = q < 0.f;
+  for (int i = 1; i < n; ++i) {
+    q = (d[i] - x) - e2[i - 1] / q;
+    if (fabsf(q) < pivmin) q = -pivmin;
+    c += q < 0.f;
+  }
+  return c;
+}
+
+// k-th smallest eigenvalue (0-based) of the tridiagonal; called by a whole warp.
+__device__ float warp_kth(const float* d, const float* e2, int n, int k, float lo, float hi, float pivmin,
+                          float abstol) {
+  const int lane = threadIdx.x & 31;
+  for (int it = 0; it < 10; ++it) {
+    const float width = hi - lo;
+    const float tol = fmaxf(2.f * FLT_EPSILON * fmaxf(fabsf(lo), fabsf(hi)), abstol);
+    if (!(width > tol)) break;
+    const float x = lo + width * ((float)(lane + 1) * (1.f / 33.f));
+    const int c = sturm_count(d, e2, n, x, pivmin);
+    const float clo = (c <= k) ? x : lo;
+    const float chi = (c > k) ? x : hi;
+    lo = warp_max(clo);
+    hi = warp_min(chi);
+    if (hi < lo) hi = lo;
+  }
+  return 0.5f * (lo + hi);
+}
+
+struct TriInfo {
+  float gl, gu, pivmin, abstol, tnorm;
+};
+
+// Eigenvalues at indices idx[0..cnt) into out[]; warps take entries.
+__device__ void cta_eigs(const float* d, const float* e2, int n, const TriInfo& ti, const int* idx,
+                         float* out, int cnt) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = warp; q < cnt; q += EIG_NW) {
+    const float v = warp_kth(d, e2, n, idx[q], ti.gl, ti.gu, ti.pivmin, ti.abstol);
+    if (lane == 0) out[q] = v;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Reference shrinkers (space_time/lowrank.py:250-280), FP64, NaN -> 0 applied
+// by the caller as at :398.
+// ---------------------------------------------------------------------------
+__device__ double opt_loss_x(double y, double beta) {
+  const double t = y * y - beta - 1.0;
+  const double v = sqrt(0.5 * (t + sqrt(t * t - 4.0 * beta)));
+  return v * ((y >= 1.0 + sqrt(beta)) ? 1.0 : 0.0);
+}
+__device__ double shrink(int loss, double y, double beta) {
+  if (loss == PD_LOSS_OPE) {
+    const double x = opt_loss_x(y, beta);
+    return isnan(x) ? x : fmax(x, 0.0);
+  }
+  if (loss == PD_LOSS_NUC) {
+    const double x = opt_loss_x(y, beta);
+    const double num = x * x * x * x - sqrt(beta) * x * y - beta;
+    const double top = isnan(num) ? num : fmax(0.0, num);
+    return top / (x * x * y);
+  }
+  const double t = (y * y - beta - 1.0);
+  const double q = t * t - 4.0 * beta;
+  return sqrt(fmax(q, 0.0) / y);
+}
+
+// ---------------------------------------------------------------------------
+// The kernel
+// ---------------------------------------------------------------------------
+template <bool CPLX>
+__global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchWork w, int in_smem) {
+  using T = typename Elem<CPLX>::T;
+  extern __shared__ __align__(16) unsigned char sm[];
+  const EigLayout L = eig_layout(CPLX, n, in_smem != 0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int p = blockIdx.x;
+  T* G = reinterpret_cast<T*>(w.gram + (int64_t)p * w.gram_stride);
+  T* A = in_smem ? reinterpret_cast<T*>(sm + L.a) : G;
+  float* d = reinterpret_cast<float*>(sm + L.d);
+  float* e = reinterpret_cast<float*>(sm + L.e);
+  float* e2 = reinterpret_cast<float*>(sm + L.e2);
+  T* tau = reinterpret_cast<T*>(sm + L.tau);
+  T* vb = reinterpret_cast<T*>(sm + L.vb);
+  T* wb = reinterpret_cast<T*>(sm + L.wb);
+  int* idx = reinterpret_cast<int*>(sm + L.idx);
+  float* lam = reinterpret_cast<float*>(sm + L.lam);
+  int* aidx = reinterpret_cast<int*>(sm + L.aidx);
+  float* alam = reinterpret_cast<float*>(sm + L.alam);
+  float* acoef = reinterpret_cast<float*>(sm + L.acoef);
+  __shared__ int s_cnt, s_act, s_c0, s_c1;
+  __shared__ double s_scale_true;  // 1/sc: true eigenvalue = scaled * this
+  __shared__ double s_x0;
+
+  const int64_t np = pk_size(n);
+  if (in_smem) {
+    for (int64_t i = tid; i < np; i += EIG_THREADS) A[i] = G[i];
+    __syncthreads();
+  }
+  // scale by 1 / max diagonal
+  float md = 0.f;
+  for (int i = tid; i < n; i += EIG_THREADS) md = fmaxf(md, re(A[pk(i, i, n)]));
+  md = bmax_f(md);
+  const float sc = md > 0.f ? 1.f / md : 1.f;
+  if (tid == 0) s_scale_true = md > 0.f ? (double)md : 1.0;
+  __syncthreads();
+  for (int64_t i = tid; i < np; i += EIG_THREADS) A[i] = A[i] * sc;
+  __syncthreads();
+
+  tridiagonalize<CPLX>(A, n, d, e, tau, vb, wb);
+
+  // e2, Gershgorin bounds, tolerances
+  float glo = FLT_MAX, ghi = -FLT_MAX, emax = 0.f, tn = 0.f;
+  for (int i = tid; i < n; i += EIG_THREADS) {
+    const float el = i > 0 ? fabsf(e[i - 1]) : 0.f;
+    const float er = i < n - 1 ? fabsf(e[i]) : 0.f;
+    if (i < n - 1) e2[i] = e[i] * e[i];
+    glo = fminf(glo, d[i] - el - er);
+    ghi = fmaxf(ghi, d[i] + el + er);
+    emax = fmaxf(emax, er * er);
+    tn = fmaxf(tn, fabsf(d[i]) + el + er);
+  }
+  glo = -bmax_f(-glo);
+  ghi = bmax_f(ghi);
+  emax = bmax_f(emax);
+  tn = bmax_f(tn);
+  TriInfo ti;
+  ti.tnorm = tn;
+  ti.pivmin = FLT_MIN * fmaxf(1.f, emax);
+  ti.abstol = 0.5f * FLT_EPSILON * tn;
+  ti.gl = glo - 2.f * FLT_EPSILON * tn - ti.pivmin;
+  ti.gu = ghi + 2.f * FLT_EPSILON * tn + ti.pivmin;
+  __syncthreads();
+
+  const double tscale = s_scale_true;  // true = scaled * tscale
+  const double M = (double)ep.rows, pt = (double)ep.cols;
+
+  // ---------------------------------------------------------------- decisions
+  if (ep.method == EIG_MODE_TOP1) {
+    if (tid == 0) idx[0] = n - 1;
+    __syncthreads();
+    cta_eigs(d, e2, n, ti, idx, lam, 1);
+    if (tid == 0) {
+      w.prior[p] = (double)lam[0] * tscale;
+      w.n_active[p] = 0;
+    }
+    return;
+  }
+
+  if (ep.method == PD_METHOD_MPPCA || ep.method == PD_METHOD_HYBRID) {
+    const int ne = n < 10 ? n : 10;
+    if (tid < ne) idx[tid] = n - ne + tid;
+    __syncthreads();
+    cta_eigs(d, e2, n, ti, idx, lam, ne);
+    if (tid == 0) {
+      double l[10];
+      for (int i = 0; i < 10; ++i) l[i] = 0.0;
+      // ascending top eigenvalues of C / (M - 1); zero-padded if n < 10
+      for (int i = 0; i < ne; ++i) l[10 - ne + i] = (double)lam[i] * tscale / (M - 1.0);
+      int k = 0;
+      double var;
+      if (ep.method == PD_METHOD_MPPCA) {
+        double s = 0.0;
+        for (int i = 0; i < 10; ++i) s += l[i];
+        double crit = (s / 10.0) * (4.0 * sqrt((10.0 - 0 + 1.0) / M));
+        while (k < 10 && crit < l[9 - k] - l[0]) {
+          ++k;
+          if (k < 10) {
+            double t = 0.0;
+            for (int i = 0; i < 10 - k; ++i) t += l[i];
+            crit = (t / (10 - k)) * (4.0 * sqrt((pt - k + 1.0) / M));
+          } else {
+            crit = nan("");
+          }
+        }
+        if (k < 10) {
+          double t = 0.0;
+          for (int i = 0; i < 10 - k; ++i) t += l[i];
+          var = t / (10 - k);
+        } else {
+          var = nan("");
+        }
+        const double cut = var * ep.threshold_scale * ep.threshold_scale;
+        int r = 0;
+        for (int i = 0; i < 10; ++i) r += (l[i] > cut) ? 1 : 0;
+        k = r;
+      } else {
+        const double varest = w.prior[p];
+        double s = 0.0;
+        for (int i = 0; i < 10; ++i) s += l[i];
+        var = s / 10.0;
+        while (var > varest && k < 10 - 2) {
+          ++k;
+          double t = 0.0;
+          for (int i = 0; i < 10 - k; ++i) t += l[i];
+          var = t / (10 - k);
+        }
+      }
+      w.rank[p] = k;
+      w.noise[p] = (float)var;
+      const int act = k < ne ? k : ne;
+      for (int a = 0; a < act; ++a) {
+        aidx[a] = n - 1 - a;  // descending eigenvalue order
+        alam[a] = lam[ne - 1 - a];
+        acoef[a] = 1.f;
+      }
+      s_act = act;
+    }
+    __syncthreads();
+  } else if (ep.method == PD_METHOD_RAW) {
+    if (tid == 0) {
+      const double x = ep.threshold * ep.threshold / tscale;  // scaled threshold on eigenvalues
+      s_c0 = sturm_count(d, e2, n, (float)(x * (1.0 - CAND_MARGIN)), ti.pivmin);
+    }
+    __syncthreads();
+    const int nc = n - s_c0;
+    for (int i = tid; i < nc; i += EIG_THREADS) idx[i] = s_c0 + i;
+    __syncthreads();
+    cta_eigs(d, e2, n, ti, idx, lam, nc);
+    if (tid == 0) {
+      int r = 0;
+      for (int i = nc - 1; i >= 0; --i) {
+        const double s = sqrt(fmax((double)lam[i] * tscale, 0.0));
+        if (s > ep.threshold) {
+          aidx[r] = idx[i];
+          alam[r] = lam[i];
+          acoef[r] = 1.f;
+          ++r;
+        }
+      }
+      w.rank[p] = r;
+      w.noise[p] = nanf("");
+      s_act = r;
+    }
+    __syncthreads();
+  } else {  // PD_METHOD_OPTIMAL
+    if (tid == 0) {
+      if (n & 1) {
+        idx[0] = (n - 1) / 2;
+        s_cnt = 1;
+      } else {
+        idx[0] = n / 2 - 1;
+        idx[1] = n / 2;
+        s_cnt = 2;
+      }
+    }
+    __syncthreads();
+    cta_eigs(d, e2, n, ti, idx, lam, s_cnt);
+    if (tid == 0) {
+      double smed;
+      if (n & 1)
+        smed = sqrt(fmax((double)lam[0] * tscale, 0.0));
+      else
+        smed = 0.5 * (sqrt(fmax((double)lam[0] * tscale, 0.0)) + sqrt(fmax((double)lam[1] * tscale, 0.0)));
+      const double sigma = ep.has_prior ? w.prior[p] : smed / sqrt(pt * ep.mp_median);
+      const double scale = sqrt(pt) * sigma;
+      const double beta = pt / M;
+      s_x0 = scale;
+      const double hi = scale * (1.0 + sqrt(beta));
+      const double lo = scale * (1.0 - sqrt(beta));
+      s_c0 = n - sturm_count(d, e2, n, (float)(hi * hi / tscale * (1.0 - CAND_MARGIN)), ti.pivmin);
+      int nb = 0;
+      if (ep.loss == PD_LOSS_FRO && lo > 0.0)
+        nb = sturm_count(d, e2, n, (float)(lo * lo / tscale * (1.0 + CAND_MARGIN)), ti.pivmin);
+      if (nb > n - s_c0) nb = n - s_c0;
+      s_c1 = nb;
+    }
+    __syncthreads();
+    const int ntop = s_c0, nbot = s_c1;
+    for (int i = tid; i < nbot; i += EIG_THREADS) idx[i] = i;
+    for (int i = tid; i < ntop; i += EIG_THREADS) idx[nbot + i] = n - ntop + i;
+    __syncthreads();
+    cta_eigs(d, e2, n, ti, idx, lam, nbot + ntop);
+    if (tid == 0) {
+      const double scale = s_x0;
+      const double beta = pt / M;
+      int act = 0, maxidx = 0;
+      for (int q = nbot + ntop - 1; q >= 0; --q) {  // descending eigenvalue order
+        const double s = sqrt(fmax((double)lam[q] * tscale, 0.0));
+        double sh = scale * shrink(ep.loss, s / scale, beta);
+        if (isnan(sh)) sh = 0.0;
+        if (sh != 0.0) {
+          aidx[act] = idx[q];
+          alam[act] = lam[q];
+          acoef[act] = (float)(sh / s);
+          ++act;
+          const int desc = n - 1 - idx[q];
+          if (desc + 1 > maxidx) maxidx = desc + 1;
+        }
+      }
+      w.rank[p] = maxidx;
+      w.noise[p] = nanf("");
+      s_act = act;
+    }
+    __syncthreads();
+  }
+
+  // ------------------------------------------------------------ eigenvectors
+  const int act = s_act;
+  const int n2 = 2 * n;
+  float* vbase = w.vec + (int64_t)p * w.vec_stride;
+  for (int a = tid; a < act; a += EIG_THREADS) {
+    float* z = vbase + (int64_t)a * n2;  // z[0..n): vector (first D-)
+    float* Dp = z + n;                   // D+ scratch
+    const float lm = alam[a];
+    const float pv = ti.pivmin;
+    float q = d[0] - lm;
+    if (fabsf(q) < pv) q = -pv;
+    Dp[0] = q;
+    for (int i = 1; i < n; ++i) {
+      q = (d[i] - lm) - e2[i - 1] / q;
+      if (fabsf(q) < pv) q = -pv;
+      Dp[i] = q;
+    }
+    q = d[n - 1] - lm;
+    if (fabsf(q) < pv) q = -pv;
+    z[n - 1] = q;
+    for (int i = n - 2; i >= 0; --i) {
+      q = (d[i] - lm) - e2[i] / q;
+      if (fabsf(q) < pv) q = -pv;
+      z[i] = q;
+    }
+    int r = 0;
+    float best = FLT_MAX;
+    for (int i = 0; i < n; ++i) {
+      const float gm = fabsf(Dp[i] + z[i] - (d[i] - lm));
+      if (gm < best) {
+        best = gm;
+        r = i;
+      }
+    }
+    z[r] = 1.f;
+    for (int i = r + 1; i < n; ++i) z[i] = -(e[i - 1] / z[i]) * z[i - 1];
+    for (int i = r - 1; i >= 0; --i) z[i] = -(e[i] / Dp[i]) * z[i + 1];
+    float s2 = 0.f;
+    for (int i = 0; i < n; ++i) s2 += z[i] * z[i];
+    const float inv = rsqrtf(s2);
+    for (int i = 0; i < n; ++i) z[i] *= inv;
+  }
+  __syncthreads();
+
+  // re-orthogonalise inside clusters (descending order; rare)
+  {
+    const float ortol = 1e-3f * ti.tnorm;
+    int cstart = 0;
+    for (int a = 1; a < act; ++a) {
+      if (alam[a - 1] - alam[a] > ortol) {
+        cstart = a;
+        continue;
+      }
+      float* za = vbase + (int64_t)a * n2;
+      for (int b = cstart; b < a; ++b) {
+        const float* zb = vbase + (int64_t)b * n2;
+        float part = 0.f;
+        for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * zb[i];
+        const float dt = bsum_f(part);
+        for (int i = tid; i < n; i += EIG_THREADS) za[i] -= dt * zb[i];
+        __syncthreads();
+      }
+      float part = 0.f;
+      for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * za[i];
+      float nr = sqrtf(bsum_f(part));
+      if (nr < 0.05f) {
+        // collapsed: inverse iteration from a pseudo-random start, orthogonalised
+        const float* Dp = za + n;
+        for (int it = 0; it < 3; ++it) {
+          if (it == 0)
+            for (int i = tid; i < n; i += EIG_THREADS) {
+              uint32_t h = (uint32_t)(i + 1) * 2654435761u ^ (uint32_t)(a + 7) * 40503u;
+              h ^= h >> 13;
+              h *= 0x5bd1e995u;
+              h ^= h >> 15;
+              za[i] = (float)(h & 0xffff) / 65536.f - 0.5f;
+            }
+          __syncthreads();
+          for (int b = cstart; b < a; ++b) {
+            const float* zb = vbase + (int64_t)b * n2;
+            float pp = 0.f;
+            for (int i = tid; i < n; i += EIG_THREADS) pp += za[i] * zb[i];
+            const float dt = bsum_f(pp);
+            for (int i = tid; i < n; i += EIG_THREADS) za[i] -= dt * zb[i];
+            __syncthreads();
+          }
+          if (tid == 0) {  // solve (T - lam I) x = za with T - lam I = L D L^T
+            for (int i = 1; i < n; ++i) za[i] -= (e[i - 1] / Dp[i - 1]) * za[i - 1];
+            for (int i = 0; i < n; ++i) za[i] /= Dp[i];
+            for (int i = n - 2; i >= 0; --i) za[i] -= (e[i] / Dp[i]) * za[i + 1];
+          }
+          __syncthreads();
+          float pp = 0.f;
+          for (int i = tid; i < n; i += EIG_THREADS) pp += za[i] * za[i];
+          const float iv = rsqrtf(bsum_f(pp));
+          for (int i = tid; i < n; i += EIG_THREADS) za[i] *= iv;
+          __syncthreads();
+        }
+        for (int b = cstart; b < a; ++b) {
+          const float* zb = vbase + (int64_t)b * n2;
+          float pp = 0.f;
+          for (int i = tid; i < n; i += EIG_THREADS) pp += za[i] * zb[i];
+          const float dt = bsum_f(pp);
+          for (int i = tid; i < n; i += EIG_THREADS) za[i] -= dt * zb[i];
+          __syncthreads();
+        }
+        part = 0.f;
+        for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * za[i];
+        nr = sqrtf(bsum_f(part));
+      }
+      const float iv = nr > 0.f ? 1.f / nr : 0.f;
+      for (int i = tid; i < n; i += EIG_THREADS) za[i] *= iv;
+      __syncthreads();
+    }
+  }
+
+  // back-transform: y = H_0 H_1 ... H_{n-2} z, one warp per vector
+  for (int a = warp; a < act; a += EIG_NW) {
+    float* col = vbase + (int64_t)a * n2;
+    T y[MAX_SLOTS];
+#pragma unroll
+    for (int s = 0; s < MAX_SLOTS; ++s) {
+      const int i = lane + 32 * s;
+      float zv = i < n ? col[i] : 0.f;
+      if constexpr (CPLX) y[s] = cf{zv, 0.f};
+      else y[s] = zv;
+    }
+    for (int j = n - 2; j >= 0; --j) {
+      const T tj = tau[j];
+      if (abs2(tj) == 0.f) continue;
+      T part = zero<T>();
+#pragma unroll
+      for (int s = 0; s < MAX_SLOTS; ++s) {
+        const int i = lane + 32 * s;
+        if (i >= j + 1 && i < n) {
+          T v;
+          if (i == j + 1) {
+            if constexpr (CPLX) v = cf{1.f, 0.f};
+            else v = 1.f;
+          } else {
+            v = A[pk(i, j, n)];
+          }
+          part = part + cmulc(v, y[s]);
+        }
+      }
+      const T dt = mul(tj, warp_sum(part));
+#pragma unroll
+      for (int s = 0; s < MAX_SLOTS; ++s) {
+        const int i = lane + 32 * s;
+        if (i >= j + 1 && i < n) {
+          T v;
+          if (i == j + 1) {
+            if constexpr (CPLX) v = cf{1.f, 0.f};
+            else v = 1.f;
+          } else {
+            v = A[pk(i, j, n)];
+          }
+          y[s] = y[s] - mul(v, dt);
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < MAX_SLOTS; ++s) {
+      const int i = lane + 32 * s;
+      if (i < n) {
+        if constexpr (CPLX) reinterpret_cast<cf*>(col)[i] = y[s];
+        else col[i] = y[s];
+      }
+    }
+  }
+  for (int a = tid; a < act; a += EIG_THREADS) w.coef[(int64_t)p * n + a] = acoef[a];
+  if (tid == 0) w.n_active[p] = act;
+}
+
+cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
+  bool in_smem;
+  const size_t smem = eig_smem_bytes(cplx, n, &in_smem);
+  cudaError_t err;
+  if (cplx) {
+    err = cudaFuncSetAttribute(k_eig<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    PD_TIMED("eig", s, k_eig<true><<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, in_smem ? 1 : 0));
+  } else {
+    err = cudaFuncSetAttribute(k_eig<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    PD_TIMED("eig", s, k_eig<false><<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, in_smem ? 1 : 0));
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace pd

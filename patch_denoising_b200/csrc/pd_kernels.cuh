@@ -1,0 +1,82 @@
+// Launchers shared between the kernel translation units and the C ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pd_common.cuh"
+
+namespace pd {
+
+constexpr int SEL_THREADS = 256;
+constexpr int SEL_PER_THREAD = 4;
+constexpr int SEL_BLOCK = SEL_THREADS * SEL_PER_THREAD;
+
+// pd_select.cu
+__global__ void k_window_counts(Geo g, const uint8_t* mask4, int32_t* cnt);
+__global__ void k_patch_flags(Geo g, int mode, const uint8_t* mask3, const int32_t* cnt, double thr,
+                              uint8_t* flags);
+__global__ void k_block_counts(const uint8_t* flags, int64_t n, int32_t* bc);
+__global__ void k_scan_counts(int32_t* bc, int64_t nb, int32_t* total_out);
+__global__ void k_compact(const uint8_t* flags, int64_t n, const int32_t* boff, int32_t* list);
+
+// Per-patch work buffers for one chunk of listed patches.
+struct PatchWork {
+  const int32_t* list;  // linear patch indices of the chunk
+  int32_t count;        // patches in the chunk
+  float* mean;          // [count][n] (complex: 2n floats)
+  float* gram;          // [count][gram_stride] packed lower Gram
+  int64_t gram_stride;  // floats per patch
+  float* vec;           // [count][vec_stride] active eigenvectors, column a at a*2n floats
+  int64_t vec_stride;   // floats per patch (2 n n)
+  float* coef;          // [count][n] synthesis coefficients
+  int32_t* n_active;    // [count]
+  int32_t* rank;        // [count] maxidx
+  float* noise;         // [count] noise_var (NaN if none)
+  double* prior;        // [count] hybrid varest / optimal sigma prior
+};
+
+// pd_gram.cu
+void launch_patch_mean(const Geo& g, bool cplx, const void* in, const PatchWork& w, cudaStream_t s);
+void launch_prior(const Geo& g, int method, const double* noise_std, const PatchWork& w, cudaStream_t s);
+void launch_gram_fp32(const Geo& g, bool cplx, const void* in, const PatchWork& w, cudaStream_t s);
+
+// pd_eig.cu
+struct EigParams {
+  int method;  // PD_METHOD_* or EIG_MODE_TOP1 (MC threshold)
+  int loss;
+  int has_prior;
+  int rows;  // M
+  int cols;  // frames
+  double threshold_scale;
+  double threshold;
+  double mp_median;
+};
+constexpr int EIG_MODE_TOP1 = 100;
+cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s);
+size_t eig_smem_bytes(bool cplx, int n, bool* in_smem);
+
+// pd_synth.cu
+struct SynthArgs {
+  int recombination;
+  void* out;            // accumulation volume (float or complex)
+  float* weight_acc;    // [nvox * gt]
+  float* noise_acc;     // [nvox * gt]
+  float* noise_ctr;     // 4D
+  int32_t* rank_map;    // 4D
+  int32_t* patch_rank;  // per listed patch (global list position)
+  float* patch_noise;
+  int64_t list_offset;  // position of the chunk inside the full list
+};
+void launch_synth(const Geo& g, bool cplx, const void* in, const PatchWork& w, const SynthArgs& a,
+                  cudaStream_t s);
+void launch_finalize(const Geo& g, bool cplx, int recombination, void* out, const float* weight_acc,
+                     const float* noise_acc, const float* noise_ctr, float* weights, float* noise_map,
+                     const uint8_t* mask, int mask_is_4d, cudaStream_t s);
+
+// pd_mc.cu
+int64_t mc_chunks(int64_t rows);
+void launch_mc_gram(int64_t rows, int cols, int n_iter, uint64_t seed, float* part, float* gram,
+                    int64_t gram_stride, cudaStream_t s);
+
+}  // namespace pd

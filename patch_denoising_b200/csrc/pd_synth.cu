@@ -1,0 +1,254 @@
+// Low-rank synthesis fused with the recombination scatter, and the final
+// normalisation / masking pass.
+//
+// For a patch with active eigenvectors V (frames x a) and coefficients c:
+//   out_r = (x_r - mean) V diag(c) V^H + mean      (row r of the Casorati matrix)
+// which equals eig_synthesis (space_time/utils.py:140-146) for c = 1 and
+// svd_synthesis with shrunk values (utils.py:81-99) for c = s~/s. The result is
+// scattered into the volume with theta = 1/(2+maxidx) (weighted), 1 (average),
+// or written at the patch centre only (center), as in base.py:243-252.
+#include <float.h>
+
+#include "pd_common.cuh"
+#include "pd_kernels.cuh"
+#include "pd_profile.cuh"
+
+namespace pd {
+
+constexpr int SYN_THREADS = 256;
+constexpr int SYN_NW = SYN_THREADS / 32;
+
+__device__ __forceinline__ void acc_add(float* p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void acc_add(cf* p, cf v) {
+  atomicAdd(reinterpret_cast<float2*>(p), make_float2(v.x, v.y));
+}
+
+template <bool CPLX, int NS, int R>
+__global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
+                                                       PatchWork w, SynthArgs sa) {
+  using T = typename Elem<CPLX>::T;
+  extern __shared__ __align__(16) unsigned char sm[];
+  const int n = g.cols, M = g.rows;
+  T* ys = reinterpret_cast<T*>(sm);  // [SYN_NW][R][n]
+  T* smean = ys + SYN_NW * R * n;    // [n]
+  float* scoef = reinterpret_cast<float*>(smean + n);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int p = blockIdx.x;
+  const int64_t pidx = w.list[p];
+  int64_t o[4];
+  patch_origin(g, pidx, o);
+  const int64_t gt = patch_window(g, pidx);
+  const int act = w.n_active[p];
+  const int rank = w.rank[p];
+  const float nv = w.noise[p];
+  const T* mean = reinterpret_cast<const T*>(w.mean) + (int64_t)p * n;
+  for (int t = tid; t < n; t += SYN_THREADS) smean[t] = mean[t];
+  for (int a = tid; a < act; a += SYN_THREADS) scoef[a] = w.coef[(int64_t)p * n + a];
+  const float* vb = w.vec + (int64_t)p * w.vec_stride;
+  const int n2 = 2 * n;
+  const int64_t T4 = g.shape[3];
+  const bool center = (sa.recombination == PD_RECOMB_CENTER);
+  const float theta = (sa.recombination == PD_RECOMB_WEIGHTED) ? (float)(1.0 / (2.0 + (double)rank)) : 1.f;
+  const int rc = (int)(((g.patch[0] / 2) * g.patch[1] + g.patch[1] / 2) * g.patch[2] + g.patch[2] / 2);
+  const int tc = (int)(g.patch[3] / 2);
+  if (blockIdx.y == 0 && tid == 0) {
+    sa.patch_rank[sa.list_offset + p] = rank;
+    sa.patch_noise[sa.list_offset + p] = nv;
+  }
+  __syncthreads();
+
+  auto vat = [&](int a, int t) -> T {
+    if constexpr (CPLX) return reinterpret_cast<const cf*>(vb + (int64_t)a * n2)[t];
+    else return vb[(int64_t)a * n2 + t];
+  };
+
+  const int rstep = gridDim.y * SYN_NW * R;
+  int r0 = (blockIdx.y * SYN_NW + warp) * R;
+  if (center) r0 = (blockIdx.y == 0 && warp == 0) ? rc : M;  // one row only
+  for (; r0 < M; r0 += center ? M : rstep) {
+    int64_t base[R];
+    bool ok[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int r = r0 + q;
+      ok[q] = (r < M) && (!center || q == 0);
+      base[q] = ok[q] ? row_voxel(g, o, r) * T4 + o[3] : 0;
+    }
+    T* yw = ys + (int64_t)warp * R * n;
+    {
+      T x[R][NS];
+#pragma unroll
+      for (int q = 0; q < R; ++q)
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const int t = lane + 32 * s;
+          x[q][s] = (ok[q] && t < n) ? in[base[q] + t] - smean[t] : zero<T>();
+        }
+      for (int a = 0; a < act; ++a) {
+        T pa[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) pa[q] = zero<T>();
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const int t = lane + 32 * s;
+          if (t < n) {
+            const T v = vat(a, t);
+#pragma unroll
+            for (int q = 0; q < R; ++q) pa[q] = pa[q] + mul(x[q][s], v);
+          }
+        }
+        const float ca = scoef[a];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const T y = warp_sum(pa[q]);
+          if (lane == 0) yw[q * n + a] = y * ca;
+        }
+      }
+    }
+    __syncwarp();
+    T ov[R][NS];
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int t = lane + 32 * s;
+        ov[q][s] = t < n ? smean[t] : zero<T>();
+      }
+    for (int a = 0; a < act; ++a) {
+      T yq[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) yq[q] = yw[q * n + a];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int t = lane + 32 * s;
+        if (t < n) {
+          const T v = cj(vat(a, t));
+#pragma unroll
+          for (int q = 0; q < R; ++q) ov[q][s] = ov[q][s] + mul(yq[q], v);
+        }
+      }
+    }
+    __syncwarp();
+    T* out = reinterpret_cast<T*>(sa.out);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      if (!ok[q]) continue;
+      if (center) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const int t = lane + 32 * s;
+          if (t == tc) out[base[q] + t] = ov[q][s];
+          if (t < n) atomicMax(&sa.rank_map[base[q] + t], rank);
+          if (t == tc && !isnan(nv)) sa.noise_ctr[base[q] + t] = nv;
+        }
+      } else {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const int t = lane + 32 * s;
+          if (t < n) acc_add(out + base[q] + t, ov[q][s] * theta);
+        }
+        if (lane == 0) {
+          const int64_t vox = (base[q] - o[3]) / T4;
+          atomicAdd(&sa.weight_acc[vox * g.grid[3] + gt], theta);
+          if (!isnan(nv)) atomicAdd(&sa.noise_acc[vox * g.grid[3] + gt], theta * nv);
+        }
+        if (r0 + q == rc) {
+#pragma unroll
+          for (int s = 0; s < NS; ++s) {
+            const int t = lane + 32 * s;
+            if (t < n) atomicMax(&sa.rank_map[base[q] + t], rank);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <bool CPLX, int NS>
+static void synth_ns(const Geo& g, const void* in, const PatchWork& w, const SynthArgs& a, cudaStream_t s) {
+  using T = typename Elem<CPLX>::T;
+  constexpr int R = CPLX ? 2 : 4;
+  const int n = g.cols;
+  const size_t smem = sizeof(T) * ((size_t)SYN_NW * R * n + n) + sizeof(float) * n + 16;
+  cudaFuncSetAttribute(k_synth<CPLX, NS, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int rows_per_block = SYN_NW * R;
+  int ysplit = (g.rows + rows_per_block - 1) / rows_per_block;
+  if (ysplit > 8) ysplit = 8;
+  if (a.recombination == PD_RECOMB_CENTER) ysplit = 1;
+  dim3 grid(w.count, ysplit);
+  PD_TIMED("synth_scatter", s, k_synth<CPLX, NS, R><<<grid, SYN_THREADS, smem, s>>>(g, (const T*)in, w, a));
+}
+
+template <bool CPLX>
+static void synth_dispatch(const Geo& g, const void* in, const PatchWork& w, const SynthArgs& a, cudaStream_t s) {
+  const int n = g.cols;
+  if (n <= 64) synth_ns<CPLX, 2>(g, in, w, a, s);
+  else if (n <= 128) synth_ns<CPLX, 4>(g, in, w, a, s);
+  else if (n <= 224) synth_ns<CPLX, 7>(g, in, w, a, s);
+  else if (n <= 320) synth_ns<CPLX, 10>(g, in, w, a, s);
+  else synth_ns<CPLX, 14>(g, in, w, a, s);
+}
+
+void launch_synth(const Geo& g, bool cplx, const void* in, const PatchWork& w, const SynthArgs& a,
+                  cudaStream_t s) {
+  if (cplx) synth_dispatch<true>(g, in, w, a, s);
+  else synth_dispatch<false>(g, in, w, a, s);
+}
+
+// out /= weights (weighted / average), expand window sums to 4D, mask.
+template <bool CPLX>
+__global__ void k_finalize(Geo g, int recomb, typename Elem<CPLX>::T* __restrict__ out,
+                           const float* __restrict__ wacc, const float* __restrict__ nacc,
+                           const float* __restrict__ nctr, float* __restrict__ weights,
+                           float* __restrict__ noise_map, const uint8_t* __restrict__ mask, int mask_is_4d) {
+  using T = typename Elem<CPLX>::T;
+  const int64_t T4 = g.shape[3];
+  const int64_t total = g.shape[0] * g.shape[1] * g.shape[2] * T4;
+  const int64_t ngt = g.grid[3];
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = e / T4, t = e % T4;
+    float wsum = 0.f, nsum = 0.f;
+    for (int64_t k = 0; k < ngt; ++k) {
+      const int64_t t0 = k * g.step[3];
+      if (t >= t0 && t < t0 + g.patch[3]) {
+        wsum += wacc[v * ngt + k];
+        nsum += nacc[v * ngt + k];
+      }
+    }
+    const bool m = mask == nullptr ? true : (mask_is_4d ? mask[e] != 0 : mask[v] != 0);
+    T val = out[e];
+    float nmap;
+    if (recomb != PD_RECOMB_CENTER) {
+      if constexpr (CPLX) val = cf{val.x / wsum, val.y / wsum};
+      else val = val / wsum;
+      nmap = nsum / wsum;
+    } else {
+      nmap = nctr[e];
+    }
+    if (!m) {
+      val = zero<T>();
+      nmap = 0.f;
+    }
+    out[e] = val;
+    weights[e] = wsum;
+    noise_map[e] = nmap;
+  }
+}
+
+void launch_finalize(const Geo& g, bool cplx, int recomb, void* out, const float* wacc, const float* nacc,
+                     const float* nctr, float* weights, float* noise_map, const uint8_t* mask, int mask_is_4d,
+                     cudaStream_t s) {
+  const int64_t total = g.shape[0] * g.shape[1] * g.shape[2] * g.shape[3];
+  int64_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (cplx)
+    PD_TIMED("finalize", s, k_finalize<true><<<(int)blocks, 256, 0, s>>>(g, recomb, (cf*)out, wacc, nacc, nctr,
+                                                                         weights, noise_map, mask, mask_is_4d));
+  else
+    PD_TIMED("finalize", s, k_finalize<false><<<(int)blocks, 256, 0, s>>>(g, recomb, (float*)out, wacc, nacc, nctr,
+                                                                          weights, noise_map, mask, mask_is_4d));
+}
+
+}  // namespace pd

@@ -1,0 +1,153 @@
+"""Low-rank denoisers (drop-in for ``patch_denoise.space_time.lowrank``).
+
+Same constructors, ``denoise`` signatures and errors as the reference classes;
+the per-patch work runs in libpd_b200.so.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from .. import _engine
+from .base import BaseSpaceTimeDenoiser, _is_float_scalar
+
+
+class MPPCADenoiser(BaseSpaceTimeDenoiser):
+    """Marchenko-Pastur PCA thresholding (space_time/lowrank.py:28-63).
+
+    ``threshold_scale`` multiplies the threshold on the eigenvalues.
+    """
+
+    _method = "mp-pca"
+
+    def __init__(self, patch_shape, patch_overlap, threshold_scale, **kwargs):
+        super().__init__(patch_shape, patch_overlap, **kwargs)
+        self.input_denoising_kwargs["threshold_scale"] = threshold_scale
+
+    def _method_args(self, data_shape, p_s, device):
+        return {"threshold_scale": float(self.input_denoising_kwargs["threshold_scale"])}
+
+
+class HybridPCADenoiser(BaseSpaceTimeDenoiser):
+    """Hybrid-PCA thresholding with a noise prior (space_time/lowrank.py:67-119)."""
+
+    _method = "hybrid-pca"
+
+    def denoise(self, input_data, mask=None, mask_threshold=50, noise_std=1.0, progbar=None):
+        """Denoise with a noise standard deviation (float or spatial map)."""
+        self.input_denoising_kwargs["noise_std"] = noise_std
+        return self._denoise(input_data, mask, mask_threshold, progbar)
+
+    def _method_args(self, data_shape, p_s, device):
+        ns = self.input_denoising_kwargs["noise_std"]
+        return {"noise_std": self._spatial_map(ns, data_shape, device)}
+
+
+class RawSVDDenoiser(BaseSpaceTimeDenoiser):
+    """Hard singular-value thresholding (space_time/lowrank.py:123-184)."""
+
+    _method = "raw"
+
+    def __init__(self, patch_shape, patch_overlap, threshold_value=1.0, recombination="weighted", **kwargs):
+        self._threshold_val = threshold_value
+        super().__init__(patch_shape, patch_overlap, recombination, **kwargs)
+
+    def denoise(self, input_data, mask=None, mask_threshold=50, threshold_scale=1.0, progbar=None):
+        """Denoise with threshold ``threshold_value * threshold_scale``."""
+        self._threshold = self._threshold_val * threshold_scale
+        return self._denoise(input_data, mask, mask_threshold, progbar)
+
+    def _method_args(self, data_shape, p_s, device):
+        return {"threshold": float(self._threshold)}
+
+
+class NordicDenoiser(RawSVDDenoiser):
+    """NORDIC: hard thresholding at a Monte-Carlo noise level (space_time/lowrank.py:188-246).
+
+    The level is ``noise_std * mean_n sigma_max(G_n)`` over ``n_iter_threshold``
+    standard Gaussian draws ``G_n`` of ``prod(patch_shape incl. time) x T``,
+    computed on the GPU (counter-based generator seeded from NumPy's global
+    generator, so ``np.random.seed`` makes a call reproducible, as in the
+    reference). ``mc_max_sval`` (extension) supplies that mean directly.
+    """
+
+    _method = "nordic"
+
+    def denoise(self, input_data, mask=None, mask_threshold=50, noise_std=1.0, n_iter_threshold=10,
+                progbar=None, mc_max_sval=None):
+        """Denoise with the NORDIC threshold."""
+        if isinstance(noise_std, np.ndarray):
+            noise_std = np.mean(noise_std)
+        if not _is_float_scalar(noise_std):
+            raise ValueError(
+                "For NORDIC the noise level must be either an"
+                " array or a float specifying the std in the volume."
+            )
+        shape = tuple(input_data.shape)
+        patch_shape, _ = self._get_patch_param(shape)
+        if mc_max_sval is None:
+            import torch
+
+            seed = int(np.random.randint(0, 2**62))
+            device = input_data.device if isinstance(input_data, torch.Tensor) and input_data.is_cuda else \
+                torch.device("cuda", torch.cuda.current_device())
+            mc_max_sval = _engine.nordic_max_sval(int(np.prod(patch_shape)), shape[-1], n_iter_threshold, seed,
+                                                  device, self.precision)
+        self.mc_max_sval_ = float(mc_max_sval)
+        self._threshold = float(noise_std) * float(mc_max_sval)
+        return self._denoise(input_data, mask, mask_threshold, progbar)
+
+
+class OptimalSVDDenoiser(BaseSpaceTimeDenoiser):
+    """Gavish-Donoho optimal shrinkage (space_time/lowrank.py:284-407).
+
+    ``loss`` is "fro", "nuc" or "ope".
+    """
+
+    _method = "optimal"
+    _LOSSES = ("fro", "nuc", "ope")
+
+    def __init__(self, patch_shape, patch_overlap, loss="fro", recombination="weighted", **kwargs):
+        super().__init__(patch_shape, patch_overlap, recombination=recombination, **kwargs)
+        if loss not in self._LOSSES:
+            raise KeyError(loss)
+        self.loss = loss
+
+    def denoise(self, input_data, mask=None, mask_threshold=50, noise_std=None, eps_marshenko_pastur=1e-7,
+                progbar=None):
+        """Denoise by optimal shrinkage; ``noise_std`` (float or map) replaces the MP estimate."""
+        shape = tuple(input_data.shape)
+        p_s, _ = self._get_patch_param(shape)
+        beta = p_s[-1] / np.prod(p_s[:-1]) if len(p_s) == len(shape) else shape[-1] / np.prod(p_s)
+        self.input_denoising_kwargs["mp_median"] = _engine.mp_median(beta, eps_marshenko_pastur)
+        self.input_denoising_kwargs["noise_std"] = noise_std
+        return self._denoise(input_data, mask, mask_threshold, progbar)
+
+    def _method_args(self, data_shape, p_s, device):
+        ns = self.input_denoising_kwargs["noise_std"]
+        return {
+            "loss": self.loss,
+            "mp_med": float(self.input_denoising_kwargs["mp_median"]),
+            "noise_std": None if ns is None else self._spatial_map(ns, data_shape, device),
+        }
+
+
+class AdaptiveDenoiser(BaseSpaceTimeDenoiser):
+    """Adaptive trace-norm shrinkage (space_time/lowrank.py:536-636).
+
+    Not part of the GPU path of this package: ``denoise`` raises.
+    """
+
+    _SUPPORTED_METHOD = ["sure", "qut", "gsure"]
+
+    def __init__(self, patch_shape, patch_overlap, method="SURE", recombination="weighted", nbsim=500):
+        super().__init__(patch_shape, patch_overlap, recombination)
+        if method.lower() not in self._SUPPORTED_METHOD:
+            raise ValueError(f"Unsupported method: '{method}', use any of {self._SUPPORTED_METHOD}")
+        self.input_denoising_kwargs["method"] = method.lower()
+        self.input_denoising_kwargs["nbsim"] = nbsim
+
+    def denoise(self, input_data, mask=None, mask_threshold=50, tau0=None, noise_std=None, gamma0=None,
+                progbar=None):
+        """Not implemented on the GPU path."""
+        raise NotImplementedError("AdaptiveDenoiser (SURE/GSURE/QUT) has no GPU implementation in this package")

@@ -1,0 +1,60 @@
+"""Shared test configuration: the ``gpu`` marker and golden-fixture helpers."""
+
+from __future__ import annotations
+
+import pathlib
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+GOLDEN = ROOT / "tests" / "golden"
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+def golden_names():
+    return sorted(p.stem for p in GOLDEN.glob("*.npz"))
+
+
+def load_golden(name):
+    """Return (arrays, call) for a fixture; ``call`` holds oracle/denoiser kwargs."""
+    z = np.load(GOLDEN / f"{name}.npz", allow_pickle=False)
+    arrays = {k: z[k] for k in z.files if not k.startswith("meta_")}
+    meta = {k[5:]: z[k] for k in z.files if k.startswith("meta_")}
+    method = str(meta["method"])
+    patch = meta["patch"]
+    overlap = meta["overlap"]
+    call = dict(
+        method=method,
+        patch_shape=int(patch) if patch.ndim == 0 else tuple(int(v) for v in patch),
+        patch_overlap=int(overlap) if overlap.ndim == 0 else tuple(int(v) for v in overlap),
+        recombination=str(meta["recombination"]),
+    )
+    if "mask" in arrays:
+        call["mask"] = arrays["mask"]
+    if "mask_threshold" in meta:
+        call["mask_threshold"] = int(meta["mask_threshold"])
+    if "threshold_scale" in meta:
+        call["threshold_scale"] = float(meta["threshold_scale"])
+    if "threshold_value" in meta:
+        call["threshold_value"] = float(meta["threshold_value"])
+    if "loss" in meta:
+        call["loss"] = str(meta["loss"])
+    if "noise_std" in arrays:
+        ns = arrays["noise_std"]
+        call["noise_std"] = float(ns) if ns.ndim == 0 else ns
+    if "seed" in meta:
+        call["seed"] = int(meta["seed"])
+    return arrays, call
+
+
+@pytest.fixture(scope="session")
+def golden():
+    return {n: load_golden(n) for n in golden_names()}

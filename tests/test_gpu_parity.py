@@ -1,0 +1,95 @@
+"""CUDA path vs the FP64 oracle (and the reference's golden outputs)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import golden_names, load_golden
+from parity import compare, rel_l2, run_ours
+from patch_denoising_b200 import _engine
+from patch_denoising_b200.synthetic import ellipsoid_mask, lowrank_volume, radial_noise_map
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_golden_case(name):
+    arrays, call = load_golden(name)
+    x = arrays["input"]
+    mc = None
+    if call["method"] == "nordic":
+        mc = float(arrays["threshold"]) / float(call.get("noise_std", 1.0))
+    res = compare(call, x, nordic_max_sval=mc)
+    # the reference's own output (float32-rounded) agrees to the same tolerance
+    (out, weights, _, _), _ = run_ours(call, x, nordic_max_sval=mc)
+    if res["ties"] == 0:
+        gold = arrays["out"]
+        np.testing.assert_array_equal(np.isnan(out), np.isnan(gold))
+        assert rel_l2(out.astype(np.complex128 if np.iscomplexobj(gold) else np.float64), gold) <= 2e-5
+        np.testing.assert_allclose(weights, arrays["weights"], rtol=1e-6)
+
+
+def test_config1_mppca_full():
+    x, _ = lowrank_volume((32, 32, 24, 60), 4, seed=1)
+    call = dict(method="mp-pca", patch_shape=5, patch_overlap=2, recombination="weighted", threshold_scale=1.0)
+    compare(call, x)
+
+
+@pytest.mark.parametrize("rec", ["weighted", "average", "center"])
+def test_config2_nordic_complex_crop(rec):
+    x, _ = lowrank_volume((28, 28, 17, 200), 6, noise=3.0, complex_valued=True, seed=2)
+    call = dict(method="nordic", patch_shape=11, patch_overlap=5, recombination=rec, noise_std=3.0)
+    compare(call, x)
+
+
+@pytest.mark.parametrize("loss", ["fro", "nuc", "ope"])
+def test_config3_optimal_masked(loss):
+    x, _ = lowrank_volume((30, 28, 20, 100), 5, noise=4.0, seed=3)
+    mask = ellipsoid_mask(x.shape[:-1], fill=0.55, seed=3)
+    call = dict(method="optimal", patch_shape=7, patch_overlap=4, recombination="weighted", loss=loss, mask=mask,
+                mask_threshold=50)
+    compare(call, x)
+
+
+def test_config4_mppca_stride1():
+    x, _ = lowrank_volume((16, 16, 16, 120), 5, noise=4.0, seed=4)
+    call = dict(method="mp-pca", patch_shape=7, patch_overlap=6, recombination="weighted", threshold_scale=1.0)
+    compare(call, x)
+
+
+def test_config5_hybrid_noise_map_crop():
+    nmap = radial_noise_map((24, 24, 14))
+    x, _ = lowrank_volume((24, 24, 14, 300), 8, noise=1.0, noise_map=nmap, seed=5)
+    call = dict(method="hybrid-pca", patch_shape=11, patch_overlap=8, recombination="weighted", noise_std=nmap)
+    compare(call, x)
+
+
+def test_config5_mppca_crop():
+    nmap = radial_noise_map((24, 24, 14))
+    x, _ = lowrank_volume((24, 24, 14, 300), 8, noise=1.0, noise_map=nmap, seed=6)
+    call = dict(method="mp-pca", patch_shape=11, patch_overlap=8, recombination="average", threshold_scale=1.0)
+    compare(call, x)
+
+
+def test_nordic_monte_carlo_level_statistics():
+    rows, cols, n = 20000, 40, 10
+    ours = _engine.nordic_max_sval(rows, cols, n, seed=7, device=torch.device("cuda", 0))
+    ref = oracle.nordic_threshold((rows,), cols, 1.0, n, np.random.RandomState(0))
+    assert abs(ours - ref) / ref < 0.01
+    # deterministic for a seed
+    again = _engine.nordic_max_sval(rows, cols, n, seed=7, device=torch.device("cuda", 0))
+    assert again == ours
+
+
+def test_torch_input_stays_on_device():
+    x, _ = lowrank_volume((20, 20, 12, 40), 3, seed=8)
+    xt = torch.from_numpy(x).cuda()
+    from patch_denoising_b200 import mp_pca
+
+    out, w, nm, rm = mp_pca(xt, 5, 2)
+    assert out.is_cuda and w.is_cuda and out.dtype == torch.float32
+    out_np, w_np, _, _ = mp_pca(x, 5, 2)
+    assert rel_l2(out.cpu().numpy().astype(np.float64), out_np.astype(np.float64)) < 1e-6

@@ -1,0 +1,126 @@
+"""Host-side logic (no GPU): C ABI exports, geometry, MP median, API surface, errors."""
+
+from __future__ import annotations
+
+import ctypes
+import itertools
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import ROOT
+from patch_denoising_b200 import _engine, _lib
+from patch_denoising_b200.bindings.utils import DENOISER_MAP, DenoiseParameters
+from patch_denoising_b200.space_time import (
+    HybridPCADenoiser,
+    MPPCADenoiser,
+    NordicDenoiser,
+    OptimalSVDDenoiser,
+    PatchedArray,
+)
+
+
+def _header_symbols():
+    text = (ROOT / "include" / "patch_denoise_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pd_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    syms = _header_symbols()
+    assert len(syms) >= 10
+    for name in syms:
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+    assert lib.pd_version() >= 100
+
+
+@pytest.mark.parametrize(
+    "shape,patch,overlap",
+    [
+        ((32, 32, 24, 60), 5, 2),
+        ((64, 64, 40, 200), 11, 5),
+        ((10, 9, 8, 20), 4, 2),
+        ((10, 9, 8, 20), (4, 4, 4, 12), (2, 2, 2, 6)),
+        ((64, 64, 20), 6, 5),
+        ((64, 64, 20), 10, 9),
+        ((30, 20), 5, 0),
+        ((12, 12, 12, 30), 12, 3),
+        ((13, 17, 19, 25), (3, 5, 7), (1, 2, 7)),
+    ],
+)
+def test_geometry_matches_oracle(shape, patch, overlap):
+    p_s, p_o = oracle.patch_params(shape, patch, overlap)
+    ps, step, grid = oracle.grid_geometry(shape, p_s, p_o)
+    g = _engine.geometry(shape, p_s, p_o)
+    pad = 4 - len(shape)
+    assert tuple(g.grid)[pad:] == grid
+    assert tuple(g.patch)[pad:] == ps
+    assert tuple(g.shape)[pad:] == shape
+    assert g.n_patches == int(np.prod(grid))
+    assert g.rows == int(np.prod(ps[:-1]))
+    assert g.cols == ps[-1]
+    # the reference's strided view has the same grid
+    view = PatchedArray(np.zeros(shape, np.float32), p_s, p_o)
+    assert view.n_patches == g.n_patches
+
+
+def test_geometry_errors():
+    with pytest.raises(ValueError, match="overlap should be smaller"):
+        _engine.geometry((10, 10, 10, 20), (4, 4, 4, 20), (5, 2, 2, 0))
+    with pytest.raises(ValueError):
+        _engine.geometry((10, 10, 10, 20), (11, 4, 4, 20), (2, 2, 2, 0))
+    with pytest.raises(NotImplementedError):
+        _engine.geometry((4, 4, 4, 4, 20), (2, 2, 2, 2, 20), (0, 0, 0, 0, 0))
+
+
+@pytest.mark.parametrize("beta", list(np.arange(1, 10) * 0.1) + [0.0, 1.0, 20 / 216, 60 / 125, 200 / 1331,
+                                                                     300 / 1331, 120 / 343])
+def test_mp_median_matches_reference_dichotomy(beta):
+    got = _engine.mp_median(beta, 1e-7)
+    ref = oracle.marchenko_pastur_median(beta, eps=1e-7)
+    # identical bracket decisions except where quad's own error flips one
+    assert abs(got - ref) <= 1e-7
+
+
+def test_mp_median_rejects_bad_beta():
+    with pytest.raises(ValueError, match="Aspect Ratio"):
+        _engine.mp_median(1.5)
+
+
+def test_denoise_parameters_roundtrip():
+    d = DenoiseParameters("optimal-fro", 11, 10, "weighted", 10)
+    d2 = DenoiseParameters.from_str(str(d))
+    assert d == d2
+    assert DenoiseParameters.from_str("noisy").method is None
+    d3 = DenoiseParameters.from_str("mp-pca_6_5_weighted")
+    assert (d3.method, d3.patch_shape, d3.patch_overlap, d3.recombination) == ("mp-pca", 6, 5, "weighted")
+
+
+def test_registry_names():
+    assert set(DENOISER_MAP) == {None, "mp-pca", "hybrid-pca", "raw", "optimal-fro", "optimal-fro-noise",
+                                 "optimal-nuc", "optimal-ope", "nordic", "adaptive-qut"}
+
+
+def test_constructor_errors():
+    with pytest.raises(ValueError, match="recombination"):
+        MPPCADenoiser(5, 2, 1.0, recombination="median")
+    with pytest.raises(KeyError):
+        OptimalSVDDenoiser(5, 2, loss="l1")
+
+
+def test_nordic_noise_std_type_error_before_device_use():
+    # space_time/lowrank.py:234-240: a non-float, non-array noise level is a ValueError
+    x = np.zeros((10, 10, 10, 20), np.float32)
+    with pytest.raises(ValueError, match="NORDIC"):
+        NordicDenoiser(4, 2).denoise(x, noise_std="not_a_float_or_array")
+
+
+def test_patch_param_int_and_tuple():
+    den = HybridPCADenoiser(6, 5)
+    assert den._get_patch_param((64, 64, 20)) == ((6, 6, 20), (5, 5, 20))
+    den = HybridPCADenoiser([3, 4, 5], (1, 1, 1))
+    assert den._get_patch_param((10, 10, 10, 30)) == ((3, 4, 5, 30), (1, 1, 1, 30))
