@@ -151,6 +151,10 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
                                  int32_t precision, double* out, void* d_workspace,
                                  size_t workspace_bytes, void* stream);
 
+/* Synchronise the stream and report whether any bounded device-side wait of the
+ * last pd_denoise_patches call on this workspace timed out (PD_ERR_CUDA). */
+pd_status pd_workspace_check(const void* d_workspace, void* stream);
+
 /* Kernel timing (no reference counterpart; used by bench.py for the roofline).
  * When enabled, every kernel launch of the library on this host thread's calls
  * is bracketed by CUDA events on its stream. pd_profile_collect synchronises

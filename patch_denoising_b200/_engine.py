@@ -177,4 +177,6 @@ def run(
         lib.pd_finalize(gp, pp, _vp(out), _vp(wacc), _vp(nacc), _vp(nctr), _vp(weights), _vp(noise_map), _vp(mask),
                         mask_4d, s)
     )
+    if n_sel:
+        _lib.check(lib.pd_workspace_check(_vp(ws), s))
     return DeviceResult(out, weights, noise_map, rank_map, plist[:n_sel], prank[:n_sel], pnoise[:n_sel])

@@ -79,6 +79,7 @@ size_t per_patch_bytes(int n, bool cplx) {
 PatchWork carve_work(void* ws, int count, int n, bool cplx, size_t* used) {
   Carver c(ws);
   PatchWork w{};
+  w.err = c.take<int>(1);  // always at offset 0 of the workspace
   w.count = count;
   w.mean = c.take<float>((size_t)count * n * (cplx ? 2 : 1));
   w.gram_stride = gram_stride_floats(n, cplx);
@@ -92,6 +93,15 @@ PatchWork carve_work(void* ws, int count, int n, bool cplx, size_t* used) {
   w.prior = c.take<double>(count);
   *used = c.off;
   return w;
+}
+
+int64_t tc_rows_per_cta(int64_t rows) {
+  int64_t r = (rows + 147) / 148;
+  return (r + 63) & ~int64_t(63);
+}
+int64_t tc_chunks(int64_t rows) {
+  const int64_t r = tc_rows_per_cta(rows);
+  return (rows + r - 1) / r;
 }
 
 size_t work_bytes(int count, int n, bool cplx) {
@@ -327,8 +337,6 @@ pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const voi
     return fail(PD_ERR_INVALID, "NULL buffer");
   if ((p->method == PD_METHOD_HYBRID || (p->method == PD_METHOD_OPTIMAL && p->has_prior)) && !d_noise_std)
     return fail(PD_ERR_INVALID, "this method needs the noise_std map");
-  if (p->precision == PD_PRECISION_MIXED)
-    return fail(PD_ERR_UNSUPPORTED, "mixed precision is not built in this library");
   const int n = (int)g->cols;
   const bool cplx = p->is_complex != 0;
   const size_t one = work_bytes(1, n, cplx);
@@ -348,6 +356,7 @@ pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const voi
   ep.threshold_scale = p->threshold_scale;
   ep.threshold = p->threshold;
   ep.mp_median = p->mp_median;
+  PD_TRY(cuda_check(cudaMemsetAsync(d_ws, 0, sizeof(int), s), "clear error word"));
   for (int64_t off = 0; off < n_selected; off += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_selected - off);
     size_t used;
@@ -356,7 +365,10 @@ pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const voi
     launch_patch_mean(G, cplx, d_in, w, s);
     if (p->method == PD_METHOD_HYBRID || (p->method == PD_METHOD_OPTIMAL && p->has_prior))
       launch_prior(G, p->method, d_noise_std, w, s);
-    launch_gram_fp32(G, cplx, d_in, w, s);
+    if (p->precision == PD_PRECISION_MIXED)
+      PD_TRY(cuda_check(launch_gram_tc(G, cplx, d_in, w, 3, w.err, s), "tensor-core Gram launch"));
+    else
+      launch_gram_fp32(G, cplx, d_in, w, s);
     PD_TRY(cuda_check(launch_eig(cplx, n, ep, w, s), "eigensolver launch"));
     SynthArgs sa;
     sa.recombination = p->recombination;
@@ -392,8 +404,10 @@ pd_status pd_nordic_workspace_size(int64_t rows, int64_t cols, int32_t n_iter, s
   if (!bytes) return fail(PD_ERR_INVALID, "NULL output");
   if (rows < 1 || cols < 1 || n_iter < 1) return fail(PD_ERR_INVALID, "empty Monte-Carlo problem");
   if (cols > MAX_FRAMES) return fail(PD_ERR_UNSUPPORTED, "at most %d frames", MAX_FRAMES);
-  *bytes = work_bytes(n_iter, (int)cols, false) +
-           align256(sizeof(float) * (size_t)n_iter * mc_chunks(rows) * pk_size((int)cols));
+  const size_t simt = align256(sizeof(float) * (size_t)n_iter * mc_chunks(rows) * pk_size((int)cols));
+  const size_t tc = align256(sizeof(float) * (size_t)rows * cols) +
+                    align256(sizeof(float) * (size_t)(tc_chunks(rows) + 1) * pk_size((int)cols));
+  *bytes = work_bytes(n_iter, (int)cols, false) + std::max(simt, tc);
   return PD_OK;
 }
 
@@ -409,8 +423,22 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
   const int n = (int)cols;
   size_t used;
   PatchWork w = carve_work(d_ws, n_iter, n, false, &used);
-  float* part = (float*)((char*)d_ws + used);
-  launch_mc_gram(rows, n, n_iter, seed, part, w.gram, w.gram_stride, s);
+  PD_TRY(cuda_check(cudaMemsetAsync(w.err, 0, sizeof(int), s), "clear error word"));
+  if (precision == PD_PRECISION_MIXED) {
+    // per draw: dense Gaussian matrix, tensor-core Gram over row chunks, ordered reduction
+    float* mat = (float*)((char*)d_ws + used);
+    float* part = (float*)((char*)mat + align256(sizeof(float) * (size_t)rows * n));
+    const int64_t rpc = tc_rows_per_cta(rows);
+    const int chunks = (int)((rows + rpc - 1) / rpc);
+    for (int d = 0; d < n_iter; ++d) {
+      launch_gauss_fill(rows, n, seed, d, mat, s);
+      PD_TRY(cuda_check(launch_dense_gram_tc(mat, rows, n, rpc, part, pk_size(n), 1, w.err, s), "Monte-Carlo Gram"));
+      launch_chunk_reduce(part, pk_size(n), chunks, pk_size(n), w.gram + (int64_t)d * w.gram_stride, s);
+    }
+  } else {
+    float* part = (float*)((char*)d_ws + used);
+    launch_mc_gram(rows, n, n_iter, seed, part, w.gram, w.gram_stride, s);
+  }
   EigParams ep{};
   ep.method = EIG_MODE_TOP1;
   ep.rows = (int)std::min<int64_t>(rows, INT32_MAX);
@@ -420,9 +448,23 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
   if (n_iter > 4096) return fail(PD_ERR_UNSUPPORTED, "at most 4096 Monte-Carlo draws");
   PD_TRY(cuda_check(cudaMemcpyAsync(lam, w.prior, sizeof(double) * n_iter, cudaMemcpyDeviceToHost, s), "copy"));
   PD_TRY(cuda_check(cudaStreamSynchronize(s), "Monte-Carlo sync"));
+  int err = 0;
+  PD_TRY(cuda_check(cudaMemcpy(&err, w.err, sizeof(int), cudaMemcpyDeviceToHost), "copy error word"));
+  if (err) return fail(PD_ERR_CUDA, "a device-side wait timed out (code %d)", err);
   double acc = 0.0;
   for (int i = 0; i < n_iter; ++i) acc += sqrt(fmax(lam[i], 0.0));
   *out = acc / n_iter;
+  return PD_OK;
+}
+
+pd_status pd_workspace_check(const void* d_workspace, void* stream) {
+  g_err.clear();
+  if (!d_workspace) return fail(PD_ERR_INVALID, "NULL workspace");
+  int err = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  PD_TRY(cuda_check(cudaMemcpyAsync(&err, d_workspace, sizeof(int), cudaMemcpyDeviceToHost, s), "copy error word"));
+  PD_TRY(cuda_check(cudaStreamSynchronize(s), "workspace check sync"));
+  if (err) return fail(PD_ERR_CUDA, "a device-side wait timed out (code %d)", err);
   return PD_OK;
 }
 

@@ -34,12 +34,19 @@ struct PatchWork {
   int32_t* rank;        // [count] maxidx
   float* noise;         // [count] noise_var (NaN if none)
   double* prior;        // [count] hybrid varest / optimal sigma prior
+  int* err;             // device error word (0 = ok)
 };
 
 // pd_gram.cu
 void launch_patch_mean(const Geo& g, bool cplx, const void* in, const PatchWork& w, cudaStream_t s);
 void launch_prior(const Geo& g, int method, const double* noise_std, const PatchWork& w, cudaStream_t s);
 void launch_gram_fp32(const Geo& g, bool cplx, const void* in, const PatchWork& w, cudaStream_t s);
+
+// pd_gram_tc.cu (tcgen05)
+cudaError_t launch_gram_tc(const Geo& g, bool cplx, const void* in, const PatchWork& w, int split, int* err,
+                           cudaStream_t s);
+cudaError_t launch_dense_gram_tc(const float* mat, int64_t rows, int cols, int64_t rows_per_cta, float* part,
+                                 int64_t part_stride, int split, int* err, cudaStream_t s);
 
 // pd_eig.cu
 struct EigParams {
@@ -76,6 +83,9 @@ void launch_finalize(const Geo& g, bool cplx, int recombination, void* out, cons
 
 // pd_mc.cu
 int64_t mc_chunks(int64_t rows);
+void launch_gauss_fill(int64_t rows, int cols, uint64_t seed, int draw, float* out, cudaStream_t s);
+void launch_chunk_reduce(const float* part, int64_t part_stride, int chunks, int64_t np, float* gram,
+                         cudaStream_t s);
 void launch_mc_gram(int64_t rows, int cols, int n_iter, uint64_t seed, float* part, float* gram,
                     int64_t gram_stride, cudaStream_t s);
 

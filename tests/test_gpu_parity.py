@@ -93,3 +93,49 @@ def test_torch_input_stays_on_device():
     assert out.is_cuda and w.is_cuda and out.dtype == torch.float32
     out_np, w_np, _, _ = mp_pca(x, 5, 2)
     assert rel_l2(out.cpu().numpy().astype(np.float64), out_np.astype(np.float64)) < 1e-6
+
+
+# ----------------------------------------------------------------- mixed precision
+@pytest.mark.parametrize("name", golden_names())
+def test_golden_case_mixed(name):
+    arrays, call = load_golden(name)
+    mc = None
+    if call["method"] == "nordic":
+        mc = float(arrays["threshold"]) / float(call.get("noise_std", 1.0))
+    compare(call, arrays["input"], precision="mixed", nordic_max_sval=mc)
+
+
+def test_config1_mppca_full_mixed():
+    x, _ = lowrank_volume((32, 32, 24, 60), 4, seed=1)
+    call = dict(method="mp-pca", patch_shape=5, patch_overlap=2, recombination="weighted", threshold_scale=1.0)
+    compare(call, x, precision="mixed")
+
+
+def test_config2_nordic_complex_crop_mixed():
+    x, _ = lowrank_volume((28, 28, 17, 200), 6, noise=3.0, complex_valued=True, seed=2)
+    call = dict(method="nordic", patch_shape=11, patch_overlap=5, recombination="weighted", noise_std=3.0)
+    compare(call, x, precision="mixed")
+
+
+@pytest.mark.parametrize("loss", ["fro", "ope"])
+def test_config3_optimal_masked_mixed(loss):
+    x, _ = lowrank_volume((30, 28, 20, 100), 5, noise=4.0, seed=3)
+    mask = ellipsoid_mask(x.shape[:-1], fill=0.55, seed=3)
+    call = dict(method="optimal", patch_shape=7, patch_overlap=4, recombination="weighted", loss=loss, mask=mask,
+                mask_threshold=50)
+    compare(call, x, precision="mixed")
+
+
+def test_config5_hybrid_noise_map_crop_mixed():
+    nmap = radial_noise_map((24, 24, 14))
+    x, _ = lowrank_volume((24, 24, 14, 300), 8, noise=1.0, noise_map=nmap, seed=5)
+    call = dict(method="hybrid-pca", patch_shape=11, patch_overlap=8, recombination="weighted", noise_std=nmap)
+    compare(call, x, precision="mixed")
+
+
+def test_nordic_monte_carlo_mixed_matches_fp32():
+    dev = torch.device("cuda", 0)
+    a = _engine.nordic_max_sval(11**3 * 200, 200, 4, seed=11, device=dev, precision="fp32")
+    b = _engine.nordic_max_sval(11**3 * 200, 200, 4, seed=11, device=dev, precision="mixed")
+    # same Gaussian draws; bf16 operands perturb the largest singular value by far less than 1e-3
+    assert abs(a - b) / a < 1e-3
