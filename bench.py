@@ -173,7 +173,7 @@ def algorithmic(kernel, n_patches, M, n, ranks):
     """(algorithmic FLOPs or bytes per call, unit kind) of a library kernel for this workload."""
     if kernel == "gram_fp32" or kernel == "gram_tc":
         return 4.0 * M * n * (n + 1) * n_patches, "flop"  # complex Hermitian rank-M update, lower triangle
-    if kernel == "mc_gram":
+    if kernel in ("mc_gram", "mc_gram_tc"):
         rows = M * n
         return float(N_ITER) * rows * n * (n + 1), "flop"
     if kernel == "synth_scatter":

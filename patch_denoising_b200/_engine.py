@@ -81,17 +81,47 @@ def compute_dtype(dtype) -> torch.dtype:
     return torch.float32
 
 
-def to_device(x, device, dtype=None, pin=False) -> torch.Tensor:
+def to_device(x, device, dtype=None) -> torch.Tensor:
+    """Host array or tensor -> contiguous device tensor of ``dtype``.
+
+    A C-contiguous NumPy array already of the compute type is page-locked in
+    place for the copy (one DMA, no staging copy) and released afterwards.
+    """
     if isinstance(x, torch.Tensor):
         t = x
-    else:
-        a = np.ascontiguousarray(x)
-        t = torch.from_numpy(a)
-        if pin:
-            t = t.pin_memory()
-    if dtype is not None and t.dtype != dtype:
-        t = t.to(dtype)
-    return t.to(device, non_blocking=pin).contiguous()
+        if dtype is not None and t.dtype != dtype:
+            t = t.to(dtype)
+        return t.to(device).contiguous()
+    a = np.ascontiguousarray(x)
+    if dtype is not None and a.dtype != _NP[dtype]:
+        a = a.astype(_NP[dtype])
+    t = torch.from_numpy(a) if a.flags.writeable else torch.from_numpy(a.copy())
+    if a.nbytes >= (1 << 20):
+        cudart = torch.cuda.cudart()
+        ptr = a.ctypes.data
+        if int(cudart.cudaHostRegister(ptr, a.nbytes, 0)) == 0:
+            try:
+                d = t.to(device, non_blocking=True)
+                torch.cuda.current_stream(device).synchronize()
+            finally:
+                cudart.cudaHostUnregister(ptr)
+            return d
+    return t.to(device)
+
+
+_NP = {torch.float32: np.float32, torch.complex64: np.complex64}
+
+
+def to_host(tensors):
+    """Device tensors -> NumPy arrays through pinned buffers (torch's host cache)."""
+    hosts = []
+    for t in tensors:
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t, non_blocking=True)
+        hosts.append(h)
+    if tensors:
+        torch.cuda.current_stream(tensors[0].device).synchronize()
+    return [h.numpy() for h in hosts]
 
 
 def run(

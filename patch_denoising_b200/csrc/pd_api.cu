@@ -425,7 +425,7 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
   PatchWork w = carve_work(d_ws, n_iter, n, false, &used);
   PD_TRY(cuda_check(cudaMemsetAsync(w.err, 0, sizeof(int), s), "clear error word"));
   if (precision == PD_PRECISION_MIXED) {
-    // per draw: dense Gaussian matrix, tensor-core Gram over row chunks, ordered reduction
+    // per draw: materialise the Gaussian matrix, tensor-core Gram over row chunks, ordered reduction
     float* mat = (float*)((char*)d_ws + used);
     float* part = (float*)((char*)mat + align256(sizeof(float) * (size_t)rows * n));
     const int64_t rpc = tc_rows_per_cta(rows);
@@ -433,7 +433,8 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
     for (int d = 0; d < n_iter; ++d) {
       launch_gauss_fill(rows, n, seed, d, mat, s);
       PD_TRY(cuda_check(launch_dense_gram_tc(mat, rows, n, rpc, part, pk_size(n), 1, w.err, s), "Monte-Carlo Gram"));
-      launch_chunk_reduce(part, pk_size(n), chunks, pk_size(n), w.gram + (int64_t)d * w.gram_stride, s);
+      launch_chunk_reduce(part, pk_size(n), chunks, pk_size(n), 1, w.gram + (int64_t)d * w.gram_stride,
+                          w.gram_stride, s);
     }
   } else {
     float* part = (float*)((char*)d_ws + used);

@@ -23,13 +23,12 @@
 
 namespace pd {
 
-constexpr int EIG_THREADS = 256;
+constexpr int EIG_THREADS = 512;
 constexpr int EIG_NW = EIG_THREADS / 32;
-constexpr int MAX_SLOTS = 14;  // n <= 448
 constexpr float CAND_MARGIN = 1e-3f;
 
 struct EigLayout {
-  size_t a, d, e, e2, tau, vb, wb, idx, lam, aidx, alam, acoef, total;
+  size_t a, d, e, e2, tau, vb, wb, pw, pd, idx, lam, aidx, alam, acoef, total;
 };
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -51,6 +50,10 @@ __host__ __device__ inline EigLayout eig_layout(bool cplx, int n, bool in_smem) 
   L.vb = o;
   o += al16(es * n);
   L.wb = o;
+  o += al16(es * n);
+  L.pw = o;
+  o += al16(es * n * (EIG_THREADS / 32));
+  L.pd = o;
   o += al16(es * n);
   L.idx = o;
   o += al16(4 * (size_t)n);
@@ -114,22 +117,74 @@ __device__ __forceinline__ float warp_min(float v) {
 
 // ---------------------------------------------------------------------------
 // Householder tridiagonalisation (lower storage, packed)
+//
+// Step j reflects column j below the subdiagonal. The symmetric product
+// p = A22 v reads each stored element of A22 once: warps own columns k, lanes
+// own rows i = lane + 32 s (registers), the row part A22(i,k) v_k accumulates in
+// registers and the transposed part sum_i conj(A22(i,k)) v_i is reduced over
+// lanes eight columns at a time (reduce-scatter butterfly, 9 shuffles).
 // ---------------------------------------------------------------------------
-template <bool CPLX>
-__device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float* e,
-                               typename Elem<CPLX>::T* tau, typename Elem<CPLX>::T* vb,
-                               typename Elem<CPLX>::T* wb) {
+template <class T>
+__device__ __forceinline__ T shfl_x(T v, int m);
+template <>
+__device__ __forceinline__ float shfl_x<float>(float v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+template <>
+__device__ __forceinline__ cf shfl_x<cf>(cf v, int m) {
+  return cf{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
+}
+
+// dp[q] (q < 8) summed over the warp; lane returns (column slot, total) with
+// slot = 4*b16 + 2*b8 + b4 valid on lanes with (lane & 3) == 0.
+template <class T>
+__device__ __forceinline__ T reduce_scatter8(const T dp[8], int lane, int* slot) {
+  const bool b16 = lane & 16, b8 = lane & 8, b4 = lane & 4;
+  T k4[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const T snd = b16 ? dp[q] : dp[q + 4];
+    const T rcv = shfl_x(snd, 16);
+    k4[q] = (b16 ? dp[q + 4] : dp[q]) + rcv;
+  }
+  T k2[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const T snd = b8 ? k4[q] : k4[q + 2];
+    const T rcv = shfl_x(snd, 8);
+    k2[q] = (b8 ? k4[q + 2] : k4[q]) + rcv;
+  }
+  const T snd = b4 ? k2[0] : k2[1];
+  const T rcv = shfl_x(snd, 4);
+  T k1 = (b4 ? k2[1] : k2[0]) + rcv;
+  k1 = k1 + shfl_x(k1, 2);
+  k1 = k1 + shfl_x(k1, 1);
+  *slot = (b16 ? 4 : 0) + (b8 ? 2 : 0) + (b4 ? 1 : 0);
+  return k1;
+}
+
+template <bool CPLX, int NS>
+__device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float* e, typename Elem<CPLX>::T* tau,
+                               typename Elem<CPLX>::T* vb, typename Elem<CPLX>::T* wb,
+                               typename Elem<CPLX>::T* pw, typename Elem<CPLX>::T* pd) {
   using T = typename Elem<CPLX>::T;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ T s_tau, s_inv;
+  __shared__ float s_xn2;
+  T one;
+  if constexpr (CPLX) one = cf{1.f, 0.f};
+  else one = 1.f;
+  // norm^2 of column 0 below the subdiagonal
+  {
+    float part = 0.f;
+    for (int i = 2 + tid; i < n; i += EIG_THREADS) part += abs2(A[pk(i, 0, n)]);
+    part = bsum_f(part);
+    if (tid == 0) s_xn2 = part;
+    __syncthreads();
+  }
   for (int j = 0; j < n - 1; ++j) {
     const int m = n - j - 1;
-    if (tid == 0) d[j] = re(A[pk(j, j, n)]);
-    // squared norm of the column below the subdiagonal element
-    float part = 0.f;
-    for (int i = j + 2 + tid; i < n; i += EIG_THREADS) part += abs2(A[pk(i, j, n)]);
-    const float xn2 = bsum_f(part);
     if (tid == 0) {
+      d[j] = re(A[pk(j, j, n)]);
+      const float xn2 = s_xn2;
       const T alpha = A[pk(j + 1, j, n)];
       const float ar = re(alpha);
       float ai = 0.f;
@@ -142,7 +197,6 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
         const float beta = ar >= 0.f ? -nrm : nrm;
         if constexpr (CPLX) {
           s_tau = cf{(beta - ar) / beta, -ai / beta};
-          // 1 / (alpha - beta)
           const float dr = ar - beta, di = ai;
           const float den = dr * dr + di * di;
           s_inv = cf{dr / den, -di / den};
@@ -156,15 +210,19 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
     }
     __syncthreads();
     const T tj = s_tau;
-    if (re(tj) == 0.f && abs2(tj) == 0.f) continue;
+    if (abs2(tj) == 0.f) {
+      // no reflection: the next column's norm still has to be formed
+      float part = 0.f;
+      for (int i = j + 3 + tid; i < n; i += EIG_THREADS) part += abs2(A[pk(i, j + 1, n)]);
+      part = bsum_f(part);
+      if (tid == 0) s_xn2 = part;
+      __syncthreads();
+      continue;
+    }
     const T inv = s_inv;
-    // v = (1, x * inv); the scaled tail is kept in A as the reflector
     for (int i = tid; i < m; i += EIG_THREADS) {
-      T v;
-      if (i == 0) {
-        if constexpr (CPLX) v = cf{1.f, 0.f};
-        else v = 1.f;
-      } else {
+      T v = one;
+      if (i > 0) {
         const int64_t q = pk(j + 1 + i, j, n);
         v = mul(A[q], inv);
         A[q] = v;
@@ -172,41 +230,88 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
       vb[i] = v;
     }
     __syncthreads();
-    // p = A22 v, lower part (k <= i): one thread per row
-    for (int i = tid; i < m; i += EIG_THREADS) {
-      T s = zero<T>();
-      const int gi = j + 1 + i;
-      for (int k = 0; k <= i; ++k) s = s + mul(A[pk(gi, j + 1 + k, n)], vb[k]);
-      wb[i] = s;
+    // ---- p = A22 v
+    {
+      T vreg[NS], acc[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int i = lane + 32 * s;
+        vreg[s] = i < m ? vb[i] : zero<T>();
+        acc[s] = zero<T>();
+      }
+      for (int k0 = warp; k0 < m; k0 += 8 * EIG_NW) {
+        T dp[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          dp[q] = zero<T>();
+          const int k = k0 + q * EIG_NW;
+          if (k < m) {
+            const T vk = vb[k];
+            const int64_t cb = pk(j + 1 + k, j + 1 + k, n) - k;  // + i gives A22(i, k)
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+              const int i = lane + 32 * s;
+              if (i >= k && i < m) {
+                const T a = A[cb + i];
+                acc[s] = acc[s] + mul(a, vk);
+                if (i > k) dp[q] = dp[q] + cmulc(a, vreg[s]);
+              }
+            }
+          }
+        }
+        int slot;
+        const T tot = reduce_scatter8<T>(dp, lane, &slot);
+        const int k = k0 + slot * EIG_NW;
+        if ((lane & 3) == 0 && k < m) pd[k] = tot;
+      }
+      T* mine = pw + (int64_t)warp * n;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < m) mine[i] = acc[s];
+      }
     }
     __syncthreads();
-    // strictly upper part: p_k += sum_{i>k} conj(A22(i,k)) v_i, one warp per column
-    for (int k = warp; k < m; k += EIG_NW) {
-      T s = zero<T>();
-      const int64_t cb = pk(j + 1 + k, j + 1 + k, n);
-      for (int i = k + 1 + lane; i < m; i += 32) s = s + cmulc(A[cb + (i - k)], vb[i]);
-      s = warp_sum(s);
-      if (lane == 0) wb[k] = wb[k] + s;
-    }
-    __syncthreads();
-    // w = tau p ; alpha2 = -tau/2 (w^H v) ; w += alpha2 v
-    T dpart = zero<T>();
-    for (int i = tid; i < m; i += EIG_THREADS) {
-      const T wi = mul(tj, wb[i]);
-      wb[i] = wi;
-      dpart = dpart + cmulc(wi, vb[i]);
+    // ---- w = tau p ; w += (-tau/2 w^H v) v
+    T wi = zero<T>(), dpart = zero<T>();
+    const int i0 = tid;
+    if (i0 < m) {
+      T p = pd[i0];
+#pragma unroll 4
+      for (int w = 0; w < EIG_NW; ++w) p = p + pw[(int64_t)w * n + i0];
+      wi = mul(tj, p);
+      dpart = cmulc(wi, vb[i0]);
     }
     const T dot = bsum<T>(dpart);
     const T a2 = mul(tj, dot) * -0.5f;
-    for (int i = tid; i < m; i += EIG_THREADS) wb[i] = wb[i] + mul(a2, vb[i]);
+    if (i0 < m) wb[i0] = wi + mul(a2, vb[i0]);
     __syncthreads();
-    // A22 -= v w^H + w v^H  (lower), one warp per column
-    for (int k = warp; k < m; k += EIG_NW) {
-      const T vk = cj(vb[k]), wk = cj(wb[k]);
-      const int64_t cb = pk(j + 1 + k, j + 1 + k, n);
-      for (int i = k + lane; i < m; i += 32) {
-        const int64_t q = cb + (i - k);
-        A[q] = A[q] - (mul(vb[i], wk) + mul(wb[i], vk));
+    // ---- A22 -= v w^H + w v^H ; norm of the next column below its subdiagonal
+    {
+      T vreg[NS], wreg[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int i = lane + 32 * s;
+        vreg[s] = i < m ? vb[i] : zero<T>();
+        wreg[s] = i < m ? wb[i] : zero<T>();
+      }
+      for (int k = warp; k < m; k += EIG_NW) {
+        const T vk = cj(vb[k]), wk = cj(wb[k]);
+        const int64_t cb = pk(j + 1 + k, j + 1 + k, n) - k;
+        float nrm = 0.f;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const int i = lane + 32 * s;
+          if (i >= k && i < m) {
+            const T a = A[cb + i] - (mul(vreg[s], wk) + mul(wreg[s], vk));
+            A[cb + i] = a;
+            if (k == 0 && i >= 2) nrm += abs2(a);
+          }
+        }
+        if (k == 0) {
+          nrm = warp_sum(nrm);
+          if (lane == 0) s_xn2 = nrm;
+        }
       }
     }
     __syncthreads();
@@ -295,7 +400,7 @@ __device__ double shrink(int loss, double y, double beta) {
 // ---------------------------------------------------------------------------
 // The kernel
 // ---------------------------------------------------------------------------
-template <bool CPLX>
+template <bool CPLX, int NS>
 __global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchWork w, int in_smem) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ __align__(16) unsigned char sm[];
@@ -310,6 +415,8 @@ __global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchW
   T* tau = reinterpret_cast<T*>(sm + L.tau);
   T* vb = reinterpret_cast<T*>(sm + L.vb);
   T* wb = reinterpret_cast<T*>(sm + L.wb);
+  T* pw = reinterpret_cast<T*>(sm + L.pw);
+  T* pd = reinterpret_cast<T*>(sm + L.pd);
   int* idx = reinterpret_cast<int*>(sm + L.idx);
   float* lam = reinterpret_cast<float*>(sm + L.lam);
   int* aidx = reinterpret_cast<int*>(sm + L.aidx);
@@ -334,7 +441,7 @@ __global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchW
   for (int64_t i = tid; i < np; i += EIG_THREADS) A[i] = A[i] * sc;
   __syncthreads();
 
-  tridiagonalize<CPLX>(A, n, d, e, tau, vb, wb);
+  tridiagonalize<CPLX, NS>(A, n, d, e, tau, vb, wb, pw, pd);
 
   // e2, Gershgorin bounds, tolerances
   float glo = FLT_MAX, ghi = -FLT_MAX, emax = 0.f, tn = 0.f;
@@ -641,9 +748,9 @@ __global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchW
   // back-transform: y = H_0 H_1 ... H_{n-2} z, one warp per vector
   for (int a = warp; a < act; a += EIG_NW) {
     float* col = vbase + (int64_t)a * n2;
-    T y[MAX_SLOTS];
+    T y[NS];
 #pragma unroll
-    for (int s = 0; s < MAX_SLOTS; ++s) {
+    for (int s = 0; s < NS; ++s) {
       const int i = lane + 32 * s;
       float zv = i < n ? col[i] : 0.f;
       if constexpr (CPLX) y[s] = cf{zv, 0.f};
@@ -654,7 +761,7 @@ __global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchW
       if (abs2(tj) == 0.f) continue;
       T part = zero<T>();
 #pragma unroll
-      for (int s = 0; s < MAX_SLOTS; ++s) {
+      for (int s = 0; s < NS; ++s) {
         const int i = lane + 32 * s;
         if (i >= j + 1 && i < n) {
           T v;
@@ -669,7 +776,7 @@ __global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchW
       }
       const T dt = mul(tj, warp_sum(part));
 #pragma unroll
-      for (int s = 0; s < MAX_SLOTS; ++s) {
+      for (int s = 0; s < NS; ++s) {
         const int i = lane + 32 * s;
         if (i >= j + 1 && i < n) {
           T v;
@@ -685,7 +792,7 @@ __global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchW
     }
     __syncwarp();
 #pragma unroll
-    for (int s = 0; s < MAX_SLOTS; ++s) {
+    for (int s = 0; s < NS; ++s) {
       const int i = lane + 32 * s;
       if (i < n) {
         if constexpr (CPLX) reinterpret_cast<cf*>(col)[i] = y[s];
@@ -697,20 +804,27 @@ __global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchW
   if (tid == 0) w.n_active[p] = act;
 }
 
-cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
+template <bool CPLX, int NS>
+static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
   bool in_smem;
-  const size_t smem = eig_smem_bytes(cplx, n, &in_smem);
-  cudaError_t err;
-  if (cplx) {
-    err = cudaFuncSetAttribute(k_eig<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
-    PD_TIMED("eig", s, k_eig<true><<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, in_smem ? 1 : 0));
-  } else {
-    err = cudaFuncSetAttribute(k_eig<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
-    PD_TIMED("eig", s, k_eig<false><<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, in_smem ? 1 : 0));
-  }
+  const size_t smem = eig_smem_bytes(CPLX, n, &in_smem);
+  cudaError_t err = cudaFuncSetAttribute(k_eig<CPLX, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  PD_TIMED("eig", s, k_eig<CPLX, NS><<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, in_smem ? 1 : 0));
   return cudaGetLastError();
+}
+
+template <bool CPLX>
+static cudaError_t eig_dispatch(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
+  if (n <= 64) return eig_ns<CPLX, 2>(n, ep, w, s);
+  if (n <= 128) return eig_ns<CPLX, 4>(n, ep, w, s);
+  if (n <= 224) return eig_ns<CPLX, 7>(n, ep, w, s);
+  if (n <= 320) return eig_ns<CPLX, 10>(n, ep, w, s);
+  return eig_ns<CPLX, 14>(n, ep, w, s);
+}
+
+cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
+  return cplx ? eig_dispatch<true>(n, ep, w, s) : eig_dispatch<false>(n, ep, w, s);
 }
 
 }  // namespace pd

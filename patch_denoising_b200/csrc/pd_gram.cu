@@ -127,6 +127,12 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_gram_fp32(Geo g, const typenam
     }
     __syncthreads();
     const T(*Bp)[GT] = diag ? As : Bs;
+    // two-level sum: the 16 rows of this step, then the running total
+    T part[4][4];
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) part[x][y] = zero<T>();
 #pragma unroll
     for (int kk = 0; kk < GK; ++kk) {
       T a[4], b[4];
@@ -138,8 +144,12 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_gram_fp32(Geo g, const typenam
 #pragma unroll
       for (int x = 0; x < 4; ++x)
 #pragma unroll
-        for (int y = 0; y < 4; ++y) acc[x][y] = acc[x][y] + cmulc(a[x], b[y]);
+        for (int y = 0; y < 4; ++y) part[x][y] = part[x][y] + cmulc(a[x], b[y]);
     }
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) acc[x][y] = acc[x][y] + part[x][y];
   }
   T* C = reinterpret_cast<T*>(w.gram) + (int64_t)p * (w.gram_stride / (CPLX ? 2 : 1));
 #pragma unroll

@@ -49,6 +49,7 @@ struct TcArgs {
   int* err;
 };
 
+
 __device__ __forceinline__ void block_of(int idx, int N, int& rb, int& nb, int& ncols) {
   for (rb = 0;; ++rb) {
     const int lim = min((rb + 1) * TC_BM, N);
@@ -158,18 +159,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_gram_tc(TcArgs a) {
       }
       uint8_t* st = sm + s * stage_bytes;
       const int64_t* rbs = rowbase + s * TC_KC;
-      for (int task = ptid; task < trows * 8; task += TC_PROD) {
-        const int trow = task % trows, g8 = task / trows;
-        const bool isA = trow < TC_BM;
-        const int row = isA ? trow : trow - TC_BM;
-        const int col = isA ? rb * TC_BM + row : nb * TC_BN + row;
-        const bool colok = col < N && (isA || row < ncols);
-        float x[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int64_t base = rbs[g8 * 8 + q];
-          x[q] = (colok && base >= 0) ? __ldg(a.in + base + col) - mean_s[col] : 0.f;
-        }
+      auto store8 = [&](int row, int g8, bool isA, const float x[8]) {
         uint4 hi;
         hi.x = pack_bf16(x[0], x[1]);
         hi.y = pack_bf16(x[2], x[3]);
@@ -193,6 +183,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_gram_tc(TcArgs a) {
           lo.w = pack_bf16(l[6], l[7]);
           *reinterpret_cast<uint4*>(st + TILE_A + TILE_B + off) = lo;
         }
+      };
+      // tasks: one tile row (an X column) x 8 K rows
+      for (int task = ptid; task < trows * 8; task += TC_PROD) {
+        const int trow = task % trows, g8 = task / trows;
+        const bool isA = trow < TC_BM;
+        const int row = isA ? trow : trow - TC_BM;
+        const int col = isA ? rb * TC_BM + row : nb * TC_BN + row;
+        const bool colok = col < N && (isA || row < ncols);
+        float x[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int64_t base = rbs[g8 * 8 + q];
+          x[q] = (colok && base >= 0) ? __ldg(a.in + base + col) - mean_s[col] : 0.f;
+        }
+        store8(row, g8, isA, x);
       }
       fence_async_smem();
       mbar_arrive(&full[s]);

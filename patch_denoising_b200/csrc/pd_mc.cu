@@ -3,13 +3,12 @@
 // chunks. The largest eigenvalue of each Gram (k_eig in top-1 mode) is the
 // squared largest singular value of the draw.
 //
-// Gaussian entries are generated on the fly: Philox-4x32-10 (Salmon, Moraes,
-// Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11) keyed by
-// (seed, draw), counter (row, column/4); the 4 words give 4 normals by the
-// Box-Muller transform. Element (r, c) is a pure function of (seed, draw, r, c).
+// Gaussian entries are generated on the fly (pd_rng.cuh): element (r, c) of
+// draw d is a pure function of (seed, d, r, c).
 #include "pd_common.cuh"
 #include "pd_kernels.cuh"
 #include "pd_profile.cuh"
+#include "pd_rng.cuh"
 
 namespace pd {
 
@@ -17,40 +16,6 @@ constexpr int MC_T = 64;
 constexpr int MC_K = 16;
 constexpr int MC_THREADS = 256;
 constexpr int64_t MC_ROWS_PER_CTA = 4096;
-
-__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
-  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
-  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    const uint32_t hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
-    const uint32_t hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
-    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-    c[0] = n0;
-    c[1] = lo1;
-    c[2] = n2;
-    c[3] = lo0;
-    k0 += W0;
-    k1 += W1;
-  }
-}
-
-// 4 standard normals for (row, column group cg) of draw `draw`.
-__device__ __forceinline__ void normals4(uint64_t seed, uint32_t draw, uint64_t row, uint32_t cg, float z[4]) {
-  uint32_t c[4] = {cg, (uint32_t)row, (uint32_t)(row >> 32), draw};
-  philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    // u1 in (0, 1], u2 in [0, 1)
-    const float u1 = ((float)c[2 * h] + 1.0f) * 2.3283064365386963e-10f;
-    const float u2 = (float)c[2 * h + 1] * 2.3283064365386963e-10f;
-    const float rad = sqrtf(-2.0f * logf(u1));
-    float sn, cs;
-    sincospif(2.0f * u2, &sn, &cs);
-    z[2 * h] = rad * cs;
-    z[2 * h + 1] = rad * sn;
-  }
-}
 
 __device__ __forceinline__ void mc_tile_pair(int t, int& bi, int& bj) {
   int i = (int)((sqrtf(8.f * t + 1.f) - 1.f) * 0.5f);
@@ -158,10 +123,10 @@ void launch_gauss_fill(int64_t rows, int cols, uint64_t seed, int draw, float* o
   PD_TIMED("gauss_fill", s, k_gauss_fill<<<(unsigned)blocks, 256, 0, s>>>(rows, cols, seed, (uint32_t)draw, out));
 }
 
-void launch_chunk_reduce(const float* part, int64_t part_stride, int chunks, int64_t np, float* gram,
-                         cudaStream_t s) {
-  dim3 rgrid((unsigned)((np + 255) / 256), 1);
-  PD_TIMED("mc_reduce", s, k_mc_reduce<<<rgrid, 256, 0, s>>>(part, part_stride, chunks, np, gram, np));
+void launch_chunk_reduce(const float* part, int64_t part_stride, int chunks, int64_t np, int draws, float* gram,
+                         int64_t gram_stride, cudaStream_t s) {
+  dim3 rgrid((unsigned)((np + 255) / 256), draws);
+  PD_TIMED("mc_reduce", s, k_mc_reduce<<<rgrid, 256, 0, s>>>(part, part_stride, chunks, np, gram, gram_stride));
 }
 
 void launch_mc_gram(int64_t rows, int cols, int n_iter, uint64_t seed, float* part, float* gram,

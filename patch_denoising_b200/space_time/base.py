@@ -149,13 +149,12 @@ class BaseSpaceTimeDenoiser(abc.ABC):
             if in_dtype in (torch.float64, torch.complex128):
                 out = out.to(in_dtype)
             return out, res.weights, res.noise_map, res.rank_map
-        out = res.out.cpu().numpy()
+        out, weights, noise_map, rank_map, pidx, prank, pnoise = _engine.to_host(
+            [res.out, res.weights, res.noise_map, res.rank_map, res.patch_index, res.patch_rank, res.patch_noise])
         if np.dtype(in_dtype) != out.dtype:
             out = out.astype(in_dtype)
-        self.patch_index_ = res.patch_index.cpu().numpy()
-        self.patch_rank_ = res.patch_rank.cpu().numpy()
-        self.patch_noise_ = res.patch_noise.cpu().numpy()
-        return out, res.weights.cpu().numpy(), res.noise_map.cpu().numpy(), res.rank_map.cpu().numpy()
+        self.patch_index_, self.patch_rank_, self.patch_noise_ = pidx, prank, pnoise
+        return out, weights, noise_map, rank_map
 
     @staticmethod
     def _device_mask(mask, data_shape, device):
