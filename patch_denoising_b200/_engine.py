@@ -82,11 +82,7 @@ def compute_dtype(dtype) -> torch.dtype:
 
 
 def to_device(x, device, dtype=None) -> torch.Tensor:
-    """Host array or tensor -> contiguous device tensor of ``dtype``.
-
-    A C-contiguous NumPy array already of the compute type is page-locked in
-    place for the copy (one DMA, no staging copy) and released afterwards.
-    """
+    """Host array or tensor -> contiguous device tensor of ``dtype``."""
     if isinstance(x, torch.Tensor):
         t = x
         if dtype is not None and t.dtype != dtype:
@@ -96,16 +92,6 @@ def to_device(x, device, dtype=None) -> torch.Tensor:
     if dtype is not None and a.dtype != _NP[dtype]:
         a = a.astype(_NP[dtype])
     t = torch.from_numpy(a) if a.flags.writeable else torch.from_numpy(a.copy())
-    if a.nbytes >= (1 << 20):
-        cudart = torch.cuda.cudart()
-        ptr = a.ctypes.data
-        if int(cudart.cudaHostRegister(ptr, a.nbytes, 0)) == 0:
-            try:
-                d = t.to(device, non_blocking=True)
-                torch.cuda.current_stream(device).synchronize()
-            finally:
-                cudart.cudaHostUnregister(ptr)
-            return d
     return t.to(device)
 
 

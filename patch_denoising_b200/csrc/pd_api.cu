@@ -63,10 +63,10 @@ int64_t gram_stride_floats(int n, bool cplx) {
 }
 int64_t vec_stride_floats(int n) { return ((int64_t)2 * n * n + 63) & ~int64_t(63); }
 
-size_t per_patch_bytes(int n, bool cplx) {
+size_t per_patch_bytes(int n, bool cplx, size_t packed = 0) {
   Carver c(nullptr);
   // carve one patch worth of every buffer (upper bound incl. alignment)
-  size_t b = 0;
+  size_t b = packed;
   b += (size_t)n * (cplx ? 8 : 4);                  // mean
   b += (size_t)gram_stride_floats(n, cplx) * 4;     // gram
   b += (size_t)vec_stride_floats(n) * 4;            // vec
@@ -76,11 +76,12 @@ size_t per_patch_bytes(int n, bool cplx) {
   return b;
 }
 
-PatchWork carve_work(void* ws, int count, int n, bool cplx, size_t* used) {
+PatchWork carve_work(void* ws, int count, int n, bool cplx, size_t* used, size_t packed_per_patch = 0) {
   Carver c(ws);
   PatchWork w{};
   w.err = c.take<int>(1);  // always at offset 0 of the workspace
   w.count = count;
+  w.packed = packed_per_patch ? (void*)c.take<uint8_t>(packed_per_patch * count) : nullptr;
   w.mean = c.take<float>((size_t)count * n * (cplx ? 2 : 1));
   w.gram_stride = gram_stride_floats(n, cplx);
   w.gram = c.take<float>((size_t)count * w.gram_stride);
@@ -104,10 +105,15 @@ int64_t tc_chunks(int64_t rows) {
   return (rows + r - 1) / r;
 }
 
-size_t work_bytes(int count, int n, bool cplx) {
+size_t work_bytes(int count, int n, bool cplx, size_t packed_per_patch = 0) {
   size_t used;
-  carve_work(nullptr, count, n, cplx, &used);
+  carve_work(nullptr, count, n, cplx, &used, packed_per_patch);
   return used;
+}
+
+size_t packed_of(const pd_geometry* g, const pd_params* p) {
+  return p->precision == PD_PRECISION_MIXED ? packed_bytes_per_patch((int)g->cols, p->is_complex != 0, (int)g->rows)
+                                            : 0;
 }
 
 pd_status check_geometry(const pd_geometry* g) {
@@ -317,10 +323,11 @@ pd_status pd_denoise_workspace_size(const pd_geometry* g, const pd_params* p, in
   if (n_selected < 0) return fail(PD_ERR_INVALID, "negative patch count");
   const int n = (int)g->cols;
   const bool cplx = p->is_complex != 0;
-  const size_t pp = per_patch_bytes(n, cplx);
+  const size_t pk_b = packed_of(g, p);
+  const size_t pp = per_patch_bytes(n, cplx, pk_b);
   int64_t chunk = (int64_t)std::max<size_t>(1, DEFAULT_CHUNK_BUDGET / pp);
   chunk = std::min<int64_t>(chunk, std::max<int64_t>(n_selected, 1));
-  *bytes = work_bytes((int)chunk, n, cplx);
+  *bytes = work_bytes((int)chunk, n, cplx, pk_b);
   return PD_OK;
 }
 
@@ -339,12 +346,13 @@ pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const voi
     return fail(PD_ERR_INVALID, "this method needs the noise_std map");
   const int n = (int)g->cols;
   const bool cplx = p->is_complex != 0;
-  const size_t one = work_bytes(1, n, cplx);
+  const size_t pk_b = packed_of(g, p);
+  const size_t one = work_bytes(1, n, cplx, pk_b);
   if (!d_ws || ws_bytes < one) return fail(PD_ERR_WORKSPACE, "workspace too small (%zu < %zu)", ws_bytes, one);
   // largest chunk that fits
-  int64_t chunk = std::max<int64_t>(1, (int64_t)(ws_bytes / per_patch_bytes(n, cplx)));
+  int64_t chunk = std::max<int64_t>(1, (int64_t)(ws_bytes / per_patch_bytes(n, cplx, pk_b)));
   chunk = std::min<int64_t>(chunk, n_selected);
-  while (chunk > 1 && work_bytes((int)chunk, n, cplx) > ws_bytes) --chunk;
+  while (chunk > 1 && work_bytes((int)chunk, n, cplx, pk_b) > ws_bytes) --chunk;
   cudaStream_t s = (cudaStream_t)stream;
   const Geo G = to_geo(*g);
   EigParams ep;
@@ -360,13 +368,13 @@ pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const voi
   for (int64_t off = 0; off < n_selected; off += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_selected - off);
     size_t used;
-    PatchWork w = carve_work(d_ws, cnt, n, cplx, &used);
+    PatchWork w = carve_work(d_ws, cnt, n, cplx, &used, pk_b);
     w.list = d_patch_list + off;
     launch_patch_mean(G, cplx, d_in, w, s);
     if (p->method == PD_METHOD_HYBRID || (p->method == PD_METHOD_OPTIMAL && p->has_prior))
       launch_prior(G, p->method, d_noise_std, w, s);
     if (p->precision == PD_PRECISION_MIXED)
-      PD_TRY(cuda_check(launch_gram_tc(G, cplx, d_in, w, 3, w.err, s), "tensor-core Gram launch"));
+      PD_TRY(cuda_check(launch_gram_packed(G, cplx, d_in, w, w.packed, s), "tensor-core Gram launch"));
     else
       launch_gram_fp32(G, cplx, d_in, w, s);
     PD_TRY(cuda_check(launch_eig(cplx, n, ep, w, s), "eigensolver launch"));
@@ -405,8 +413,8 @@ pd_status pd_nordic_workspace_size(int64_t rows, int64_t cols, int32_t n_iter, s
   if (rows < 1 || cols < 1 || n_iter < 1) return fail(PD_ERR_INVALID, "empty Monte-Carlo problem");
   if (cols > MAX_FRAMES) return fail(PD_ERR_UNSUPPORTED, "at most %d frames", MAX_FRAMES);
   const size_t simt = align256(sizeof(float) * (size_t)n_iter * mc_chunks(rows) * pk_size((int)cols));
-  const size_t tc = align256(sizeof(float) * (size_t)rows * cols) +
-                    align256(sizeof(float) * (size_t)(tc_chunks(rows) + 1) * pk_size((int)cols));
+  const size_t tc = align256(gauss_packed_bytes(rows, (int)cols, n_iter)) +
+                    align256(sizeof(float) * (size_t)n_iter * gauss_chunks(rows, (int)cols) * pk_size((int)cols));
   *bytes = work_bytes(n_iter, (int)cols, false) + std::max(simt, tc);
   return PD_OK;
 }
@@ -425,17 +433,13 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
   PatchWork w = carve_work(d_ws, n_iter, n, false, &used);
   PD_TRY(cuda_check(cudaMemsetAsync(w.err, 0, sizeof(int), s), "clear error word"));
   if (precision == PD_PRECISION_MIXED) {
-    // per draw: materialise the Gaussian matrix, tensor-core Gram over row chunks, ordered reduction
-    float* mat = (float*)((char*)d_ws + used);
-    float* part = (float*)((char*)mat + align256(sizeof(float) * (size_t)rows * n));
-    const int64_t rpc = tc_rows_per_cta(rows);
-    const int chunks = (int)((rows + rpc - 1) / rpc);
-    for (int d = 0; d < n_iter; ++d) {
-      launch_gauss_fill(rows, n, seed, d, mat, s);
-      PD_TRY(cuda_check(launch_dense_gram_tc(mat, rows, n, rpc, part, pk_size(n), 1, w.err, s), "Monte-Carlo Gram"));
-      launch_chunk_reduce(part, pk_size(n), chunks, pk_size(n), 1, w.gram + (int64_t)d * w.gram_stride,
-                          w.gram_stride, s);
-    }
+    // generate the draws packed as bf16 G^T, TMA-fed tensor-core Gram over K chunks, ordered reduction
+    void* packed = (char*)d_ws + used;
+    float* part = (float*)((char*)packed + align256(gauss_packed_bytes(rows, n, n_iter)));
+    const int chunks = (int)gauss_chunks(rows, n);
+    PD_TRY(cuda_check(launch_gauss_gram_packed(rows, n, n_iter, seed, packed, part, pk_size(n), w.err, s),
+                      "Monte-Carlo Gram"));
+    launch_chunk_reduce(part, pk_size(n), chunks, pk_size(n), n_iter, w.gram, w.gram_stride, s);
   } else {
     float* part = (float*)((char*)d_ws + used);
     launch_mc_gram(rows, n, n_iter, seed, part, w.gram, w.gram_stride, s);
@@ -470,3 +474,8 @@ pd_status pd_workspace_check(const void* d_workspace, void* stream) {
 }
 
 }  // extern "C"
+
+namespace pd {
+// Sets the message pd_last_error() returns on this host thread.
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace pd

@@ -1,0 +1,430 @@
+// Mixed-precision Gram, operands packed once and fed to tcgen05 by TMA.
+//
+// k_pack_patches: for every listed patch, the centred Casorati matrix X (M rows
+//   x N real columns; a complex patch is its interleaved real view, N = 2 n) is
+//   written transposed as two bf16 matrices Xhi^T, Xlo^T (N rows x Kp, Kp = M
+//   rounded up to 64, zero padded), x = hi + lo to about 16 bits. Reads are
+//   coalesced along frames, writes along voxels through a shared-memory
+//   transpose; the kernel is memory bound and runs at full occupancy.
+// k_gauss_pack: the same layout for the NORDIC Monte-Carlo draws (bf16 hi only),
+//   generating the normals of (seed, draw, row, column) directly.
+// k_gram_tma: CTA = (patch or row chunk, 128 x <=256 block of the lower Gram).
+//   One thread issues cp.async.bulk.tensor loads (128-byte swizzle, the
+//   canonical K-major layout of tcgen05) into a 2-stage ring guarded by
+//   mbarriers with transaction counts; one thread issues tcgen05.mma with the
+//   accumulator in TMEM (hi*hi + hi*lo + lo*hi, or hi*hi for the draws);
+//   four warps read TMEM and write the packed Gram (complex via 2x2 blocks).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "pd_common.cuh"
+#include "pd_kernels.cuh"
+#include "pd_profile.cuh"
+#include "pd_rng.cuh"
+#include "pd_tc.cuh"
+
+namespace pd {
+
+constexpr int PK_R = 64;  // K rows per pack tile
+constexpr int PK_C = 64;  // columns per pack tile
+constexpr int TM_BM = 128;
+constexpr int TM_BN = 256;
+constexpr int TM_BOX = 128;  // rows per TMA box
+constexpr int TM_STAGES = 2;
+constexpr int TM_THREADS = 128;
+constexpr uint32_t TM_TILE_A = TM_BM * 128;
+constexpr uint32_t TM_TILE_B = TM_BN * 128;
+
+__host__ __device__ inline int64_t pack_k(int64_t rows) { return (rows + 63) & ~int64_t(63); }
+
+// ---------------------------------------------------------------------------
+// Packing
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pack_store(__nv_bfloat16* hi, __nv_bfloat16* lo, int64_t off, float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  *reinterpret_cast<__nv_bfloat162*>(hi + off) = h;
+  if (lo) {
+    const float2 f = __bfloat1622float2(h);
+    *reinterpret_cast<__nv_bfloat162*>(lo + off) = __floats2bfloat162_rn(a - f.x, b - f.y);
+  }
+}
+
+// grid: (patches, Kp / 64, ceil(N / 64)), 256 threads.
+__global__ void __launch_bounds__(256) k_pack_patches(Geo g, const float* __restrict__ in, int N, int cplx,
+                                                      const float* __restrict__ mean, const int32_t* __restrict__ list,
+                                                      __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
+                                                      int64_t kp) {
+  __shared__ float tile[PK_R][PK_C + 1];
+  __shared__ int64_t rb[PK_R];
+  const int p = blockIdx.x;
+  const int r0 = blockIdx.y * PK_R, c0 = blockIdx.z * PK_C;
+  const int tid = threadIdx.x;
+  int64_t o[4];
+  patch_origin(g, list[p], o);
+  if (tid < PK_R) {
+    const int r = r0 + tid;
+    rb[tid] = r < g.rows ? (row_voxel(g, o, r) * g.shape[3] + o[3]) * (cplx ? 2 : 1) : -1;
+  }
+  __syncthreads();
+  const int c = tid % PK_C;
+  const int col = c0 + c;
+  const float mu = col < N ? mean[(int64_t)p * N + col] : 0.f;
+#pragma unroll 4
+  for (int rr = tid / PK_C; rr < PK_R; rr += 256 / PK_C) {
+    const int64_t base = rb[rr];
+    tile[rr][c] = (base >= 0 && col < N) ? __ldg(in + base + col) - mu : 0.f;
+  }
+  __syncthreads();
+  // each warp writes 64 K-values (128 B) of a column per step
+  const int warp = tid >> 5, lane = tid & 31;
+  __nv_bfloat16* hp = hi + (int64_t)p * N * kp;
+  __nv_bfloat16* lp = lo ? lo + (int64_t)p * N * kp : nullptr;
+  for (int cc = warp; cc < PK_C; cc += 8) {
+    const int colw = c0 + cc;
+    if (colw >= N) break;
+    const int64_t off = (int64_t)colw * kp + r0 + 2 * lane;
+    pack_store(hp, lp, off, tile[2 * lane][cc], tile[2 * lane + 1][cc]);
+  }
+}
+
+// Gaussian draws, packed transposed: G^T[d][c][r] for r < rows (zero to kp).
+// grid: (kp / 64, ceil(cols / 64), draws), 256 threads.
+__global__ void __launch_bounds__(256) k_gauss_pack(int64_t rows, int cols, uint64_t seed,
+                                                    __nv_bfloat16* __restrict__ out, int64_t kp) {
+  __shared__ float tile[PK_R][PK_C + 1];
+  const int64_t r0 = (int64_t)blockIdx.x * PK_R;
+  const int c0 = blockIdx.y * PK_C;
+  const int d = blockIdx.z;
+  const int tid = threadIdx.x;
+  // 64 rows x 16 column groups of 4 = 1024 Philox blocks, 4 per thread
+  for (int t = tid; t < PK_R * (PK_C / 4); t += 256) {
+    const int rr = t / (PK_C / 4), cg = t % (PK_C / 4);
+    const int64_t r = r0 + rr;
+    const int col = c0 + cg * 4;
+    float z[4] = {0.f, 0.f, 0.f, 0.f};
+    if (r < rows && col < cols) normals4(seed, (uint32_t)d, (uint64_t)r, (uint32_t)(col >> 2), z);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) tile[rr][cg * 4 + q] = (col + q < cols) ? z[q] : 0.f;
+  }
+  __syncthreads();
+  const int warp = tid >> 5, lane = tid & 31;
+  __nv_bfloat16* op = out + (int64_t)d * cols * kp;
+  for (int cc = warp; cc < PK_C; cc += 8) {
+    const int colw = c0 + cc;
+    if (colw >= cols) break;
+    pack_store(op, nullptr, (int64_t)colw * kp + r0 + 2 * lane, tile[2 * lane][cc], tile[2 * lane + 1][cc]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// TMA + tcgen05 Gram
+// ---------------------------------------------------------------------------
+struct TmaArgs {
+  int N;       // real columns of X (= rows of the packed operand)
+  int n_out;   // output order (N or N/2 for complex)
+  int cplx;
+  int split;   // 3: hi/lo, 1: hi only
+  int64_t kp;  // packed K extent
+  int dense;   // 1: blockIdx.x is a K chunk of one operand per blockIdx.z
+  int64_t k_per_cta;
+  float* out;
+  int64_t out_stride;
+  int* err;
+};
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tm_block_of(int idx, int N, int& rb, int& nb, int& ncols) {
+  for (rb = 0;; ++rb) {
+    const int lim = min((rb + 1) * TM_BM, N);
+    const int nbs = (lim + TM_BN - 1) / TM_BN;
+    if (idx < nbs) {
+      nb = idx;
+      ncols = min(lim - nb * TM_BN, TM_BN);
+      return;
+    }
+    idx -= nbs;
+  }
+}
+
+__global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constant__ CUtensorMap map_hi,
+                                                             const __grid_constant__ CUtensorMap map_lo, TmaArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int N = a.N;
+  const bool split = a.split == 3;
+  const uint32_t stage_bytes = (split ? 2u : 1u) * (TM_TILE_A + TM_TILE_B);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + TM_STAGES * stage_bytes);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + TM_STAGES;
+  uint64_t* done = bars + 2 * TM_STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+
+  int rb, nb, ncols;
+  tm_block_of(blockIdx.y, N, rb, nb, ncols);
+  const int npad = (ncols + 15) & ~15;
+  const int nbox = (npad + TM_BOX - 1) / TM_BOX;  // B boxes of 128 rows
+  uint32_t tcols = 32;
+  while (tcols < (uint32_t)npad) tcols <<= 1;
+
+  int64_t k_begin = 0, k_end = a.kp;
+  int zc = blockIdx.x;  // third tensor-map coordinate: patch, or draw
+  float* out;
+  if (a.dense) {
+    k_begin = (int64_t)blockIdx.x * a.k_per_cta;
+    k_end = min(k_begin + a.k_per_cta, a.kp);
+    zc = blockIdx.z;
+    out = a.out + ((int64_t)blockIdx.z * gridDim.x + blockIdx.x) * a.out_stride;
+  } else {
+    out = a.out + (int64_t)blockIdx.x * a.out_stride;
+  }
+  const int nch = (int)((k_end - k_begin + 63) / 64);
+  const uint32_t tx_bytes = (split ? 2u : 1u) * (TM_TILE_A + (uint32_t)nbox * TM_BOX * 128u);
+
+  if (tid == 0) {
+    for (int s = 0; s < TM_STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    mbar_fence_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, tcols);
+    tc_fence_before();
+  }
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t taddr = *tmem_slot;
+  const uint32_t sbase = smem_u32(sm);
+
+  if (warp == 0 && lane == 0) {
+    // ------------------------------------------------------------ TMA producer
+    for (int c = 0; c < nch; ++c) {
+      const int s = c % TM_STAGES;
+      if (c >= TM_STAGES && !mbar_wait(&empty[s], ((c / TM_STAGES) - 1) & 1)) {
+        atomicExch(a.err, 4);
+        break;
+      }
+      const uint32_t st = sbase + s * stage_bytes;
+      const uint32_t fb = smem_u32(&full[s]);
+      mbar_expect_tx(&full[s], tx_bytes);
+      const int kc = (int)(k_begin + (int64_t)c * 64);
+      tma_load_3d(st, &map_hi, kc, rb * TM_BM, zc, fb);
+      for (int q = 0; q < nbox; ++q) tma_load_3d(st + TM_TILE_A + q * TM_BOX * 128, &map_hi, kc, nb * TM_BN + q * TM_BOX, zc, fb);
+      if (split) {
+        const uint32_t lo = st + TM_TILE_A + TM_TILE_B;
+        tma_load_3d(lo, &map_lo, kc, rb * TM_BM, zc, fb);
+        for (int q = 0; q < nbox; ++q) tma_load_3d(lo + TM_TILE_A + q * TM_BOX * 128, &map_lo, kc, nb * TM_BN + q * TM_BOX, zc, fb);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ------------------------------------------------------------ MMA issuer
+    const uint32_t idesc = umma_idesc_bf16(npad);
+    for (int c = 0; c < nch; ++c) {
+      const int s = c % TM_STAGES;
+      if (!mbar_wait(&full[s], (c / TM_STAGES) & 1)) {
+        atomicExch(a.err, 5);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t st = sbase + s * stage_bytes;
+      const uint32_t ahi = st, bhi = st + TM_TILE_A, alo = st + TM_TILE_A + TM_TILE_B, blo = alo + TM_TILE_A;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t kb = k * 32;
+        const uint64_t da = umma_desc_sw128(ahi + kb), db = umma_desc_sw128(bhi + kb);
+        umma_bf16(taddr, da, db, idesc, (c | k) != 0 ? 1u : 0u);
+        if (split) {
+          umma_bf16(taddr, da, umma_desc_sw128(blo + kb), idesc, 1u);
+          umma_bf16(taddr, umma_desc_sw128(alo + kb), db, idesc, 1u);
+        }
+      }
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);
+  }
+  __syncwarp();
+
+  // ------------------------------------------------------------ epilogue (4 warps)
+  const bool ok = mbar_wait(done, 0);
+  __syncwarp();
+  tc_fence_after();
+  if (!ok && lane == 0) atomicExch(a.err, 6);
+  const int i = rb * TM_BM + warp * 32 + lane;
+  const uint32_t lane_addr = taddr + ((uint32_t)(warp * 32) << 16);
+  for (int cc = 0; cc < npad; cc += 16) {
+    float v[16];
+    tmem_ld16(lane_addr + cc, v);
+    if (!a.cplx) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int j = nb * TM_BN + cc + q;
+        if (ok && i < N && j <= i && (cc + q) < ncols) out[pk(i, j, N)] = v[q];
+      }
+    } else {
+      float vp[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) vp[q] = __shfl_xor_sync(0xffffffffu, v[q], 1);
+      if ((i & 1) == 0) {
+        const int ic = i >> 1, n = a.n_out;
+        cf* oc = reinterpret_cast<cf*>(out);
+#pragma unroll
+        for (int q = 0; q < 16; q += 2) {
+          const int jc = (nb * TM_BN + cc + q) >> 1;
+          if (ok && ic < n && jc <= ic && (cc + q) < ncols) oc[pk(ic, jc, n)] = cf{v[q] + vp[q + 1], v[q + 1] - vp[q]};
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(taddr, tcols);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+std::mutex g_enc_mu;
+EncodeFn g_encode = nullptr;
+
+cudaError_t get_encode(EncodeFn* fn) {
+  std::lock_guard<std::mutex> lk(g_enc_mu);
+  if (!g_encode) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return e;
+    if (q != cudaDriverEntryPointSuccess || !p) return cudaErrorNotSupported;
+    g_encode = reinterpret_cast<EncodeFn>(p);
+  }
+  *fn = g_encode;
+  return cudaSuccess;
+}
+
+// 3D bf16 map: (K = kp [contiguous], rows = N, depth), box 64 x 128 x 1, 128-byte swizzle.
+cudaError_t make_map(CUtensorMap* m, const void* base, int64_t kp, int N, int64_t depth) {
+  EncodeFn enc;
+  cudaError_t e = get_encode(&enc);
+  if (e != cudaSuccess) return e;
+  cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)N, (cuuint64_t)depth};
+  cuuint64_t strides[2] = {(cuuint64_t)kp * 2, (cuuint64_t)kp * 2 * N};
+  cuuint32_t box[3] = {64, TM_BOX, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+int tm_blocks(int N) {
+  int t = 0;
+  for (int rb = 0; rb * TM_BM < N; ++rb) {
+    const int lim = (rb + 1) * TM_BM < N ? (rb + 1) * TM_BM : N;
+    t += (lim + TM_BN - 1) / TM_BN;
+  }
+  return t;
+}
+
+size_t tm_smem(int split) { return 1024 + TM_STAGES * (size_t)(split == 3 ? 2 : 1) * (TM_TILE_A + TM_TILE_B) + 64; }
+}  // namespace
+
+size_t packed_bytes_per_patch(int n, bool cplx, int M) {
+  const int N = cplx ? 2 * n : n;
+  return (size_t)2 * 2 * N * pack_k(M);  // hi + lo bf16
+}
+
+cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const PatchWork& w, void* packed,
+                               cudaStream_t s) {
+  const int N = cplx ? 2 * g.cols : g.cols;
+  const int64_t kp = pack_k(g.rows);
+  __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(packed);
+  __nv_bfloat16* lo = hi + (int64_t)w.count * N * kp;
+  dim3 pg(w.count, (unsigned)(kp / PK_R), (N + PK_C - 1) / PK_C);
+  PD_TIMED("pack", s, k_pack_patches<<<pg, 256, 0, s>>>(g, (const float*)in, N, cplx ? 1 : 0, w.mean, w.list, hi, lo, kp));
+  CUtensorMap mh, ml;
+  cudaError_t e = make_map(&mh, hi, kp, N, w.count);
+  if (e != cudaSuccess) return e;
+  e = make_map(&ml, lo, kp, N, w.count);
+  if (e != cudaSuccess) return e;
+  TmaArgs a{};
+  a.N = N;
+  a.n_out = g.cols;
+  a.cplx = cplx ? 1 : 0;
+  a.split = 3;
+  a.kp = kp;
+  a.dense = 0;
+  a.out = w.gram;
+  a.out_stride = w.gram_stride;
+  a.err = w.err;
+  const size_t smem = tm_smem(3);
+  e = cudaFuncSetAttribute(k_gram_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid(w.count, tm_blocks(N));
+  PD_TIMED("gram_tc", s, k_gram_tma<<<grid, TM_THREADS, smem, s>>>(mh, ml, a));
+  return cudaGetLastError();
+}
+
+size_t gauss_packed_bytes(int64_t rows, int cols, int n_iter) { return (size_t)2 * cols * pack_k(rows) * n_iter; }
+
+int64_t gauss_k_per_cta(int64_t rows, int cols) {
+  // about 2 waves of CTAs over the draws' row chunks
+  const int blocks = tm_blocks(cols);
+  int64_t chunks = (2 * 148 + blocks - 1) / blocks;
+  int64_t k = (pack_k(rows) + chunks - 1) / chunks;
+  return (k + 63) & ~int64_t(63);
+}
+
+cudaError_t launch_gauss_gram_packed(int64_t rows, int cols, int n_iter, uint64_t seed, void* packed, float* part,
+                                     int64_t part_stride, int* err, cudaStream_t s) {
+  const int64_t kp = pack_k(rows);
+  __nv_bfloat16* g = reinterpret_cast<__nv_bfloat16*>(packed);
+  dim3 pg((unsigned)(kp / PK_R), (cols + PK_C - 1) / PK_C, n_iter);
+  PD_TIMED("gauss_pack", s, k_gauss_pack<<<pg, 256, 0, s>>>(rows, cols, seed, g, kp));
+  CUtensorMap mh;
+  cudaError_t e = make_map(&mh, g, kp, cols, n_iter);
+  if (e != cudaSuccess) return e;
+  TmaArgs a{};
+  a.N = cols;
+  a.n_out = cols;
+  a.split = 1;
+  a.kp = kp;
+  a.dense = 1;
+  a.k_per_cta = gauss_k_per_cta(rows, cols);
+  a.out = part;
+  a.out_stride = part_stride;
+  a.err = err;
+  const size_t smem = tm_smem(1);
+  e = cudaFuncSetAttribute(k_gram_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int64_t chunks = (kp + a.k_per_cta - 1) / a.k_per_cta;
+  dim3 grid((unsigned)chunks, tm_blocks(cols), n_iter);
+  PD_TIMED("mc_gram_tc", s, k_gram_tma<<<grid, TM_THREADS, smem, s>>>(mh, mh, a));
+  return cudaGetLastError();
+}
+
+int64_t gauss_chunks(int64_t rows, int cols) {
+  const int64_t k = gauss_k_per_cta(rows, cols);
+  return (pack_k(rows) + k - 1) / k;
+}
+
+}  // namespace pd

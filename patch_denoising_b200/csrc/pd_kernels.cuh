@@ -35,6 +35,7 @@ struct PatchWork {
   float* noise;         // [count] noise_var (NaN if none)
   double* prior;        // [count] hybrid varest / optimal sigma prior
   int* err;             // device error word (0 = ok)
+  void* packed;         // mixed precision: bf16 hi/lo operands of the chunk
 };
 
 // pd_gram.cu
@@ -79,6 +80,15 @@ void launch_synth(const Geo& g, bool cplx, const void* in, const PatchWork& w, c
 void launch_finalize(const Geo& g, bool cplx, int recombination, void* out, const float* weight_acc,
                      const float* noise_acc, const float* noise_ctr, float* weights, float* noise_map,
                      const uint8_t* mask, int mask_is_4d, cudaStream_t s);
+
+// pd_gram_tma.cu (pack + TMA-fed tcgen05)
+size_t packed_bytes_per_patch(int n, bool cplx, int M);
+cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const PatchWork& w, void* packed,
+                               cudaStream_t s);
+size_t gauss_packed_bytes(int64_t rows, int cols, int n_iter);
+int64_t gauss_chunks(int64_t rows, int cols);
+cudaError_t launch_gauss_gram_packed(int64_t rows, int cols, int n_iter, uint64_t seed, void* packed, float* part,
+                                     int64_t part_stride, int* err, cudaStream_t s);
 
 // pd_mc.cu
 int64_t mc_chunks(int64_t rows);

@@ -29,7 +29,8 @@ def test_golden_case(name):
         gold = arrays["out"]
         np.testing.assert_array_equal(np.isnan(out), np.isnan(gold))
         assert rel_l2(out.astype(np.complex128 if np.iscomplexobj(gold) else np.float64), gold) <= 2e-5
-        np.testing.assert_allclose(weights, arrays["weights"], rtol=1e-6)
+        # float32 sums of up to ~100 overlapping patches in atomic (unordered) order
+        np.testing.assert_allclose(weights, arrays["weights"], rtol=1e-5)
 
 
 def test_config1_mppca_full():
