@@ -151,6 +151,22 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
                                  int32_t precision, double* out, void* d_workspace,
                                  size_t workspace_bytes, void* stream);
 
+/* pd_denoise_patches without a workspace argument. No counterpart in the
+ * reference. It is for callers that cannot allocate device memory while they
+ * denoise, e.g. a host application that manages a fixed device-memory budget
+ * itself, or a loop where cudaMalloc's implicit synchronisation is not
+ * acceptable. The scratch is a static 32 MiB device array inside the library
+ * that every GPU loading the library keeps until exit. Patches are processed
+ * in chunks that fit it. A geometry whose single-patch scratch exceeds 32 MiB
+ * returns PD_ERR_WORKSPACE. The first call on a device looks up the array's
+ * device address; make that call before any stream capture. All calls share the
+ * array, so calls that overlap on the GPU (other streams or host threads) race.
+ * Arguments are those of pd_denoise_patches minus the workspace. */
+pd_status pd_denoise_patches_noalloc(const pd_geometry* g, const pd_params* p, const void* d_in,
+                                     const double* d_noise_std, const int32_t* d_patch_list, int64_t n_selected,
+                                     void* d_out_acc, float* d_weight_acc, float* d_noise_acc, float* d_noise_ctr,
+                                     int32_t* d_rank_map, int32_t* d_patch_rank, float* d_patch_noise, void* stream);
+
 /* Synchronise the stream and report whether any bounded device-side wait of the
  * last pd_denoise_patches call on this workspace timed out (PD_ERR_CUDA). */
 pd_status pd_workspace_check(const void* d_workspace, void* stream);
