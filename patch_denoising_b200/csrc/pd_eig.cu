@@ -48,9 +48,9 @@ __host__ __device__ inline EigLayout eig_layout(bool cplx, int n, bool in_smem) 
   L.tau = o;
   o += al16(es * n);
   L.vb = o;
-  o += al16(es * n);
+  o += al16(es * 2 * n);
   L.wb = o;
-  o += al16(es * n);
+  o += al16(es * 2 * n);
   L.pw = o;
   o += al16(es * n * (EIG_THREADS / 32));
   L.pd = o;
@@ -116,14 +116,33 @@ __device__ __forceinline__ float warp_min(float v) {
 }
 
 // ---------------------------------------------------------------------------
-// Householder tridiagonalisation (lower storage, packed)
+// Householder tridiagonalisation (lower storage, packed), after LAPACK
+// zhetd2 / ssytd2 with uplo = 'L' (the reduction behind scipy's eigh): step j
+// reflects column j below the subdiagonal with H_j = I - tau_j v_j v_j^H,
+// v_j(j+1) = 1, and updates the trailing block A22 <- A22 - v w^H - w v^H with
+// p = A22 v, w = tau p + alpha v, alpha = -tau/2 (tau p)^H v.
 //
-// Step j reflects column j below the subdiagonal. The symmetric product
-// p = A22 v reads each stored element of A22 once: warps own columns k, lanes
-// own rows i = lane + 32 s (registers), the row part A22(i,k) v_k accumulates in
-// registers and the transposed part sum_i conj(A22(i,k)) v_i is reduced over
-// lanes eight columns at a time (reduce-scatter butterfly, 9 shuffles).
+// Three block barriers per step. The rank-2 update of step j-1 and the product
+// p_j = A22 v_j of step j share one pass over A22, so each stored element is
+// loaded, updated, stored and multiplied once per step; only column j, which
+// reflector j is built from, takes its update ahead of the pass (warp 0).
+//   phase 1 (warp 0): alpha_{j-1}; column j -= update_{j-1}; reflector j
+//   phase 2 (all):    A22 -= update_{j-1}; partial sums of A22 v_j: warps own
+//                     columns k, lanes own rows i = lane + 32 s (registers); the
+//                     row part A22(i,k) v_k accumulates in registers, the
+//                     transposed part sum_i conj(A22(i,k)) v_i is reduced over
+//                     lanes eight columns at a time (reduce-scatter butterfly)
+//   phase 3 (all):    p_j from the partials; tau_j p_j; partials of (tau p)^H v
+// v and tau p live in two buffers of n entries indexed by row (step parity).
 // ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ T shfl_idx(T v, int src);
+template <>
+__device__ __forceinline__ float shfl_idx<float>(float v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <>
+__device__ __forceinline__ cf shfl_idx<cf>(cf v, int src) {
+  return cf{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
+}
 template <class T>
 __device__ __forceinline__ T shfl_x(T v, int m);
 template <>
@@ -167,77 +186,108 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
                                typename Elem<CPLX>::T* pw, typename Elem<CPLX>::T* pd) {
   using T = typename Elem<CPLX>::T;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  __shared__ T s_tau, s_inv;
-  __shared__ float s_xn2;
+  __shared__ T s_red[EIG_NW];  // per-warp partials of (tau p)^H v
+  __shared__ T s_alpha;        // alpha of the previous step
+  __shared__ T s_tau;          // tau of the current step
   T one;
   if constexpr (CPLX) one = cf{1.f, 0.f};
   else one = 1.f;
-  // norm^2 of column 0 below the subdiagonal
-  {
-    float part = 0.f;
-    for (int i = 2 + tid; i < n; i += EIG_THREADS) part += abs2(A[pk(i, 0, n)]);
-    part = bsum_f(part);
-    if (tid == 0) s_xn2 = part;
-    __syncthreads();
+  // buffer 1 holds "step -1": v = w = 0, so the first pending update is exactly zero
+  for (int i = tid; i < 2 * n; i += EIG_THREADS) {
+    vb[i] = zero<T>();
+    wb[i] = zero<T>();
   }
+  if (tid < EIG_NW) s_red[tid] = zero<T>();
+  T tau_prev = zero<T>();  // warp 0: tau of the previous step
+  __syncthreads();
   for (int j = 0; j < n - 1; ++j) {
     const int m = n - j - 1;
-    if (tid == 0) {
-      d[j] = re(A[pk(j, j, n)]);
-      const float xn2 = s_xn2;
-      const T alpha = A[pk(j + 1, j, n)];
+    const int cur = j & 1;
+    T* vc = vb + cur * n;
+    T* wc = wb + cur * n;
+    const T* vp = vb + (cur ^ 1) * n;
+    const T* wp = wb + (cur ^ 1) * n;
+    // ---- phase 1 (warp 0): finish column j, build reflector j
+    if (warp == 0) {
+      T dot = lane < EIG_NW ? s_red[lane] : zero<T>();
+      dot = warp_sum(dot);
+      const T al = mul(tau_prev, dot) * -0.5f;  // w_{j-1} = tau p + al v
+      const T vj = vp[j];
+      const T cuj = cj(wp[j] + mul(al, vj)), cvj = cj(vj);
+      T col[NS];
+      float xn2 = 0.f;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int r = j + lane + 32 * s;
+        col[s] = zero<T>();
+        if (r < n) {
+          const T v = vp[r];
+          const T u = wp[r] + mul(al, v);
+          const T a = A[pk(r, j, n)] - (mul(v, cuj) + mul(u, cvj));
+          col[s] = a;
+          if (r >= j + 2) xn2 += abs2(a);
+        }
+      }
+      xn2 = warp_sum(xn2);
+      const T alpha = shfl_idx(col[0], 1);  // A(j+1, j)
       const float ar = re(alpha);
       float ai = 0.f;
       if constexpr (CPLX) ai = alpha.y;
-      if (xn2 == 0.f && ai == 0.f) {
-        s_tau = zero<T>();
-        e[j] = ar;
-      } else {
+      const bool refl = !(xn2 == 0.f && ai == 0.f);
+      T tj = zero<T>(), inv = zero<T>();
+      float ej = ar;
+      if (refl) {
         const float nrm = sqrtf(ar * ar + ai * ai + xn2);
         const float beta = ar >= 0.f ? -nrm : nrm;
         if constexpr (CPLX) {
-          s_tau = cf{(beta - ar) / beta, -ai / beta};
+          tj = cf{(beta - ar) / beta, -ai / beta};
           const float dr = ar - beta, di = ai;
           const float den = dr * dr + di * di;
-          s_inv = cf{dr / den, -di / den};
+          inv = cf{dr / den, -di / den};
         } else {
-          s_tau = (beta - ar) / beta;
-          s_inv = 1.f / (ar - beta);
+          tj = (beta - ar) / beta;
+          inv = 1.f / (ar - beta);
         }
-        e[j] = beta;
+        ej = beta;
       }
-      tau[j] = s_tau;
-    }
-    __syncthreads();
-    const T tj = s_tau;
-    if (abs2(tj) == 0.f) {
-      // no reflection: the next column's norm still has to be formed
-      float part = 0.f;
-      for (int i = j + 3 + tid; i < n; i += EIG_THREADS) part += abs2(A[pk(i, j + 1, n)]);
-      part = bsum_f(part);
-      if (tid == 0) s_xn2 = part;
-      __syncthreads();
-      continue;
-    }
-    const T inv = s_inv;
-    for (int i = tid; i < m; i += EIG_THREADS) {
-      T v = one;
-      if (i > 0) {
-        const int64_t q = pk(j + 1 + i, j, n);
-        v = mul(A[q], inv);
-        A[q] = v;
-      }
-      vb[i] = v;
-    }
-    __syncthreads();
-    // ---- p = A22 v
-    {
-      T vreg[NS], acc[NS];
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        const int i = lane + 32 * s;
-        vreg[s] = i < m ? vb[i] : zero<T>();
+        const int r = j + lane + 32 * s;
+        if (r > j && r < n) {
+          T v = zero<T>();
+          if (refl) {
+            v = (r == j + 1) ? one : mul(col[s], inv);
+            if (r > j + 1) A[pk(r, j, n)] = v;
+          }
+          vc[r] = v;
+        }
+      }
+      if (lane == 0) {
+        d[j] = re(col[0]);
+        e[j] = ej;
+        tau[j] = tj;
+        s_tau = tj;
+        s_alpha = al;
+      }
+      tau_prev = tj;
+    }
+    __syncthreads();
+    // ---- phase 2 (all): A22 -= update_{j-1}; partial sums of p = A22 v_j
+    {
+      const T al = s_alpha;
+      T vo[NS], uo[NS], vn[NS], acc[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int i = lane + 32 * s, r = j + 1 + i;
+        vo[s] = zero<T>();
+        uo[s] = zero<T>();
+        vn[s] = zero<T>();
         acc[s] = zero<T>();
+        if (i < m) {
+          vo[s] = vp[r];
+          uo[s] = wp[r] + mul(al, vo[s]);
+          vn[s] = vc[r];
+        }
       }
       for (int k0 = warp; k0 < m; k0 += 8 * EIG_NW) {
         T dp[8];
@@ -246,15 +296,21 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
           dp[q] = zero<T>();
           const int k = k0 + q * EIG_NW;
           if (k < m) {
-            const T vk = vb[k];
-            const int64_t cb = pk(j + 1 + k, j + 1 + k, n) - k;  // + i gives A22(i, k)
+            const int c = j + 1 + k;
+            const T vok = vp[c];
+            const T cvo = cj(vok), cuo = cj(wp[c] + mul(al, vok)), vk = vc[c];
+            const int cb = (int)pk(c, c, n) - k;  // + i gives A22(i, k)
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
               const int i = lane + 32 * s;
               if (i >= k && i < m) {
-                const T a = A[cb + i];
+                T a = A[cb + i] - (mul(vo[s], cuo) + mul(uo[s], cvo));
+                if constexpr (CPLX) {
+                  if (i == k) a.y = 0.f;  // Hermitian diagonal stays real
+                }
+                A[cb + i] = a;
                 acc[s] = acc[s] + mul(a, vk);
-                if (i > k) dp[q] = dp[q] + cmulc(a, vreg[s]);
+                if (i > k) dp[q] = dp[q] + cmulc(a, vn[s]);
               }
             }
           }
@@ -262,63 +318,49 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
         int slot;
         const T tot = reduce_scatter8<T>(dp, lane, &slot);
         const int k = k0 + slot * EIG_NW;
-        if ((lane & 3) == 0 && k < m) pd[k] = tot;
+        if ((lane & 3) == 0 && k < m) pd[j + 1 + k] = tot;
       }
-      T* mine = pw + (int64_t)warp * n;
+      T* mine = pw + warp * n;
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
         const int i = lane + 32 * s;
-        if (i < m) mine[i] = acc[s];
+        if (i < m) mine[j + 1 + i] = acc[s];
       }
     }
     __syncthreads();
-    // ---- w = tau p ; w += (-tau/2 w^H v) v
-    T wi = zero<T>(), dpart = zero<T>();
-    const int i0 = tid;
-    if (i0 < m) {
-      T p = pd[i0];
-#pragma unroll 4
-      for (int w = 0; w < EIG_NW; ++w) p = p + pw[(int64_t)w * n + i0];
-      wi = mul(tj, p);
-      dpart = cmulc(wi, vb[i0]);
-    }
-    const T dot = bsum<T>(dpart);
-    const T a2 = mul(tj, dot) * -0.5f;
-    if (i0 < m) wb[i0] = wi + mul(a2, vb[i0]);
-    __syncthreads();
-    // ---- A22 -= v w^H + w v^H ; norm of the next column below its subdiagonal
+    // ---- phase 3 (all): w = tau p, partials of w^H v
     {
-      T vreg[NS], wreg[NS];
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        const int i = lane + 32 * s;
-        vreg[s] = i < m ? vb[i] : zero<T>();
-        wreg[s] = i < m ? wb[i] : zero<T>();
+      const T tj = s_tau;
+      T dpart = zero<T>();
+      if (tid < m) {
+        const int r = j + 1 + tid;
+        T pv = pd[r];
+#pragma unroll 4
+        for (int w = 0; w < EIG_NW; ++w) pv = pv + pw[w * n + r];
+        const T wv = mul(tj, pv);
+        wc[r] = wv;
+        dpart = cmulc(wv, vc[r]);
       }
-      for (int k = warp; k < m; k += EIG_NW) {
-        const T vk = cj(vb[k]), wk = cj(wb[k]);
-        const int64_t cb = pk(j + 1 + k, j + 1 + k, n) - k;
-        float nrm = 0.f;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-          const int i = lane + 32 * s;
-          if (i >= k && i < m) {
-            const T a = A[cb + i] - (mul(vreg[s], wk) + mul(wreg[s], vk));
-            A[cb + i] = a;
-            if (k == 0 && i >= 2) nrm += abs2(a);
-          }
-        }
-        if (k == 0) {
-          nrm = warp_sum(nrm);
-          if (lane == 0) s_xn2 = nrm;
-        }
-      }
+      dpart = warp_sum(dpart);
+      if (lane == 0) s_red[warp] = dpart;
     }
     __syncthreads();
   }
   if (tid == 0) {
-    d[n - 1] = re(A[pk(n - 1, n - 1, n)]);
-    if (n == 1) e[0] = 0.f;
+    if (n == 1) {
+      d[0] = re(A[0]);
+      e[0] = 0.f;
+    } else {
+      // the last diagonal entry takes the update of step n-2
+      T dot = zero<T>();
+      for (int w = 0; w < EIG_NW; ++w) dot = dot + s_red[w];
+      const T al = mul(tau[n - 2], dot) * -0.5f;
+      const int c = (n - 2) & 1;
+      const T v = vb[c * n + n - 1];
+      const T u = wb[c * n + n - 1] + mul(al, v);
+      const T a = A[pk(n - 1, n - 1, n)] - (mul(v, cj(u)) + mul(u, cj(v)));
+      d[n - 1] = re(a);
+    }
   }
   __syncthreads();
 }
@@ -373,6 +415,108 @@ __device__ void cta_eigs(const float* d, const float* e2, int n, const TriInfo& 
 }
 
 // ---------------------------------------------------------------------------
+// Largest eigenvalue of a real symmetric packed matrix: the noise level of a
+// NORDIC Monte-Carlo draw (space_time/lowrank.py:222-232 averages the top
+// singular value of each Gaussian draw). Lanczos with full re-orthogonalisation
+// (two classical Gram-Schmidt passes per step) from a fixed start vector, then
+// multisection on the Lanczos tridiagonal. On the Gram of a tall Gaussian
+// matrix with 200 columns, 48 steps bring the top Ritz value to 1e-12
+// (relative) of the top eigenvalue in exact arithmetic, so with LANCZOS_STEPS
+// the FP32 result is limited by rounding alone. The matrix is scaled so that
+// its largest diagonal entry is 1, hence its top eigenvalue is >= 1.
+// ---------------------------------------------------------------------------
+constexpr int LANCZOS_STEPS = 56;
+
+// Q: (min(n, LANCZOS_STEPS) + 1) * n floats of scratch; al, be, be2: n floats each.
+__device__ float lanczos_top1(const float* A, int n, float* Q, float* al, float* be, float* be2) {
+  __shared__ float s_coef[LANCZOS_STEPS];
+  __shared__ float s_val;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int kmax = n < LANCZOS_STEPS ? n : LANCZOS_STEPS;
+  float* wv = Q + (int64_t)kmax * n;
+  float part = 0.f;
+  for (int i = tid; i < n; i += EIG_THREADS) {
+    uint32_t h = (uint32_t)(i + 7) * 2654435761u;
+    h ^= h >> 13;
+    h *= 0x5bd1e995u;
+    h ^= h >> 15;
+    const float x = 1.0f + (float)(h & 0xffff) * (1.f / 65536.f);
+    Q[i] = x;
+    part += x * x;
+  }
+  const float nr = rsqrtf(bsum_f(part));
+  for (int i = tid; i < n; i += EIG_THREADS) Q[i] *= nr;
+  __syncthreads();
+  int kk = kmax;
+  for (int j = 0; j < kmax; ++j) {
+    const float* qj = Q + (int64_t)j * n;
+    // w = A q_j: a warp per row, lanes over the columns
+    for (int r = warp; r < n; r += EIG_NW) {
+      float s = 0.f;
+      for (int k = lane; k < n; k += 32) s += A[k <= r ? pk(r, k, n) : pk(k, r, n)] * qj[k];
+      s = warp_sum(s);
+      if (lane == 0) wv[r] = s;
+    }
+    __syncthreads();
+    float b2p = 0.f;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int c = warp; c <= j; c += EIG_NW) {
+        const float* qc = Q + (int64_t)c * n;
+        float s = 0.f;
+        for (int i = lane; i < n; i += 32) s += qc[i] * wv[i];
+        s = warp_sum(s);
+        if (lane == 0) s_coef[c] = s;
+      }
+      __syncthreads();
+      if (pass == 0 && tid == 0) al[j] = s_coef[j];
+      b2p = 0.f;
+      for (int i = tid; i < n; i += EIG_THREADS) {
+        float s = wv[i];
+        for (int c = 0; c <= j; ++c) s -= s_coef[c] * Q[(int64_t)c * n + i];
+        wv[i] = s;
+        b2p += s * s;
+      }
+      __syncthreads();
+    }
+    const float b2 = bsum_f(b2p);
+    if (tid == 0) {
+      be2[j] = b2;
+      be[j] = sqrtf(b2);
+    }
+    if (j + 1 >= kmax || !(b2 > 1e-12f)) {
+      kk = j + 1;
+      break;
+    }
+    const float inv = rsqrtf(b2);
+    float* qn = Q + (int64_t)(j + 1) * n;
+    for (int i = tid; i < n; i += EIG_THREADS) qn[i] = wv[i] * inv;
+    __syncthreads();
+  }
+  __syncthreads();
+  // top eigenvalue of the kk x kk Lanczos tridiagonal (al, be)
+  if (warp == 0) {
+    float lo = FLT_MAX, hi = -FLT_MAX, emax = 0.f, tn = 0.f;
+    for (int i = lane; i < kk; i += 32) {
+      const float el = i > 0 ? be[i - 1] : 0.f, er = i < kk - 1 ? be[i] : 0.f;
+      lo = fminf(lo, al[i] - el - er);
+      hi = fmaxf(hi, al[i] + el + er);
+      emax = fmaxf(emax, er * er);
+      tn = fmaxf(tn, fabsf(al[i]) + el + er);
+    }
+    lo = -warp_max(-lo);
+    hi = warp_max(hi);
+    emax = warp_max(emax);
+    tn = warp_max(tn);
+    const float pv = FLT_MIN * fmaxf(1.f, emax);
+    const float v = warp_kth(al, be2, kk, kk - 1, lo - 2.f * FLT_EPSILON * tn - pv, hi + 2.f * FLT_EPSILON * tn + pv,
+                             pv, 0.5f * FLT_EPSILON * tn);
+    if (lane == 0) s_val = v;
+  }
+  __syncthreads();
+  return s_val;
+}
+
+// ---------------------------------------------------------------------------
 // Reference shrinkers (space_time/lowrank.py:250-280), FP64, NaN -> 0 applied
 // by the caller as at :398.
 // ---------------------------------------------------------------------------
@@ -401,7 +545,7 @@ __device__ double shrink(int loss, double y, double beta) {
 // The kernel
 // ---------------------------------------------------------------------------
 template <bool CPLX, int NS>
-__global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchWork w, int in_smem) {
+__global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, PatchWork w, int in_smem) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ __align__(16) unsigned char sm[];
   const EigLayout L = eig_layout(CPLX, n, in_smem != 0);
@@ -441,6 +585,16 @@ __global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchW
   for (int64_t i = tid; i < np; i += EIG_THREADS) A[i] = A[i] * sc;
   __syncthreads();
 
+  if constexpr (!CPLX) {
+    if (ep.method == EIG_MODE_TOP1) {  // Monte-Carlo level: top eigenvalue only
+      const float lam1 = lanczos_top1(A, n, w.vec + (int64_t)p * w.vec_stride, d, e, e2);
+      if (tid == 0) {
+        w.prior[p] = (double)lam1 * s_scale_true;
+        w.n_active[p] = 0;
+      }
+      return;
+    }
+  }
   tridiagonalize<CPLX, NS>(A, n, d, e, tau, vb, wb, pw, pd);
 
   // e2, Gershgorin bounds, tolerances
@@ -470,17 +624,6 @@ __global__ void __launch_bounds__(EIG_THREADS) k_eig(int n, EigParams ep, PatchW
   const double M = (double)ep.rows, pt = (double)ep.cols;
 
   // ---------------------------------------------------------------- decisions
-  if (ep.method == EIG_MODE_TOP1) {
-    if (tid == 0) idx[0] = n - 1;
-    __syncthreads();
-    cta_eigs(d, e2, n, ti, idx, lam, 1);
-    if (tid == 0) {
-      w.prior[p] = (double)lam[0] * tscale;
-      w.n_active[p] = 0;
-    }
-    return;
-  }
-
   if (ep.method == PD_METHOD_MPPCA || ep.method == PD_METHOD_HYBRID) {
     const int ne = n < 10 ? n : 10;
     if (tid < ne) idx[tid] = n - ne + tid;
@@ -810,7 +953,7 @@ static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaSt
   const size_t smem = eig_smem_bytes(CPLX, n, &in_smem);
   cudaError_t err = cudaFuncSetAttribute(k_eig<CPLX, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  PD_TIMED("eig", s, k_eig<CPLX, NS><<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, in_smem ? 1 : 0));
+  PD_TIMED(ep.method == EIG_MODE_TOP1 ? "eig_mc" : "eig", s, k_eig<CPLX, NS><<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, in_smem ? 1 : 0));
   return cudaGetLastError();
 }
 
