@@ -91,8 +91,37 @@ def to_device(x, device, dtype=None) -> torch.Tensor:
     a = np.ascontiguousarray(x)
     if dtype is not None and a.dtype != _NP[dtype]:
         a = a.astype(_NP[dtype])
-    t = torch.from_numpy(a) if a.flags.writeable else torch.from_numpy(a.copy())
-    return t.to(device)
+    if a.nbytes < _STAGE_MIN:
+        t = torch.from_numpy(a) if a.flags.writeable else torch.from_numpy(a.copy())
+        return t.to(device)
+    return _staged_h2d(a, device)
+
+
+# Host-to-device copies of pageable NumPy memory run through two pinned staging
+# buffers: the host copy of chunk k + 1 (torch's multi-threaded memcpy) overlaps
+# the DMA of chunk k, instead of the driver's single-threaded staging.
+_STAGE_MIN = 16 << 20
+_STAGE_CHUNK = 32 << 20
+
+
+def _staged_h2d(a: np.ndarray, device) -> torch.Tensor:
+    src = torch.from_numpy(a.reshape(-1).view(np.uint8))
+    nbytes = src.numel()
+    dst = torch.empty(nbytes, dtype=torch.uint8, device=device)
+    stream = torch.cuda.current_stream(device)
+    chunk = min(_STAGE_CHUNK, nbytes)
+    stage = [torch.empty(chunk, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    done = [None, None]
+    for k, lo in enumerate(range(0, nbytes, chunk)):
+        hi = min(lo + chunk, nbytes)
+        b = k & 1
+        if done[b] is not None:
+            done[b].synchronize()  # the DMA out of this buffer has finished
+        stage[b][: hi - lo].copy_(src[lo:hi])
+        dst[lo:hi].copy_(stage[b][: hi - lo], non_blocking=True)
+        done[b] = torch.cuda.Event()
+        done[b].record(stream)
+    return dst.view(torch.from_numpy(a[:0]).dtype).view(a.shape)
 
 
 _NP = {torch.float32: np.float32, torch.complex64: np.complex64}
