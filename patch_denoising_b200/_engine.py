@@ -183,7 +183,11 @@ def run(
         lib.pd_select_patches(gp, _vp(mask), mask_4d, float(mask_threshold), _vp(plist), _vp(count), _vp(ws),
                               need.value, s)
     )
-    n_sel = int(count.item())
+    if mask is None:
+        # every patch scores 100 % (k_patch_flags without a mask): no device round trip
+        n_sel = int(g.n_patches) if 100.0 > float(mask_threshold) else 0
+    else:
+        n_sel = int(count.item())
 
     # ---- parameters
     prm = _lib.Params()

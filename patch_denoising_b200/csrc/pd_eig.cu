@@ -420,12 +420,12 @@ __device__ void cta_eigs(const float* d, const float* e2, int n, const TriInfo& 
 // singular value of each Gaussian draw). Lanczos with full re-orthogonalisation
 // (two classical Gram-Schmidt passes per step) from a fixed start vector, then
 // multisection on the Lanczos tridiagonal. On the Gram of a tall Gaussian
-// matrix with 200 columns, 48 steps bring the top Ritz value to 1e-12
-// (relative) of the top eigenvalue in exact arithmetic, so with LANCZOS_STEPS
-// the FP32 result is limited by rounding alone. The matrix is scaled so that
+// matrix with 200 columns, 48 steps bring the top Ritz value to 1e-13
+// (relative) of the top eigenvalue in exact arithmetic, so the FP32 result
+// is limited by rounding alone. The matrix is scaled so that
 // its largest diagonal entry is 1, hence its top eigenvalue is >= 1.
 // ---------------------------------------------------------------------------
-constexpr int LANCZOS_STEPS = 56;
+constexpr int LANCZOS_STEPS = 48;
 
 // Q: (min(n, LANCZOS_STEPS) + 1) * n floats of scratch; al, be, be2: n floats each.
 __device__ float lanczos_top1(const float* A, int n, float* Q, float* al, float* be, float* be2) {
@@ -472,6 +472,7 @@ __device__ float lanczos_top1(const float* A, int n, float* Q, float* al, float*
       b2p = 0.f;
       for (int i = tid; i < n; i += EIG_THREADS) {
         float s = wv[i];
+#pragma unroll 8
         for (int c = 0; c <= j; ++c) s -= s_coef[c] * Q[(int64_t)c * n + i];
         wv[i] = s;
         b2p += s * s;
@@ -545,14 +546,16 @@ __device__ double shrink(int loss, double y, double beta) {
 // The kernel
 // ---------------------------------------------------------------------------
 template <bool CPLX, int NS>
+// in_smem: bit 0 = the packed matrix lives in shared memory, bit 1 = the
+// Lanczos basis of the top-1 mode does too (after the layout's end).
 __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, PatchWork w, int in_smem) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ __align__(16) unsigned char sm[];
-  const EigLayout L = eig_layout(CPLX, n, in_smem != 0);
+  const EigLayout L = eig_layout(CPLX, n, (in_smem & 1) != 0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int p = blockIdx.x;
   T* G = reinterpret_cast<T*>(w.gram + (int64_t)p * w.gram_stride);
-  T* A = in_smem ? reinterpret_cast<T*>(sm + L.a) : G;
+  T* A = (in_smem & 1) ? reinterpret_cast<T*>(sm + L.a) : G;
   float* d = reinterpret_cast<float*>(sm + L.d);
   float* e = reinterpret_cast<float*>(sm + L.e);
   float* e2 = reinterpret_cast<float*>(sm + L.e2);
@@ -571,7 +574,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
   __shared__ double s_x0;
 
   const int64_t np = pk_size(n);
-  if (in_smem) {
+  if (in_smem & 1) {
     for (int64_t i = tid; i < np; i += EIG_THREADS) A[i] = G[i];
     __syncthreads();
   }
@@ -587,7 +590,8 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
 
   if constexpr (!CPLX) {
     if (ep.method == EIG_MODE_TOP1) {  // Monte-Carlo level: top eigenvalue only
-      const float lam1 = lanczos_top1(A, n, w.vec + (int64_t)p * w.vec_stride, d, e, e2);
+      float* Q = (in_smem & 2) ? reinterpret_cast<float*>(sm + L.total) : w.vec + (int64_t)p * w.vec_stride;
+      const float lam1 = lanczos_top1(A, n, Q, d, e, e2);
       if (tid == 0) {
         w.prior[p] = (double)lam1 * s_scale_true;
         w.n_active[p] = 0;
@@ -950,10 +954,18 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
 template <bool CPLX, int NS>
 static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
   bool in_smem;
-  const size_t smem = eig_smem_bytes(CPLX, n, &in_smem);
+  size_t smem = eig_smem_bytes(CPLX, n, &in_smem);
+  int flags = in_smem ? 1 : 0;
+  if (!CPLX && ep.method == EIG_MODE_TOP1 && in_smem) {
+    const size_t q = al16(sizeof(float) * (size_t)((n < LANCZOS_STEPS ? n : LANCZOS_STEPS) + 1) * n);
+    if (smem + q <= EIG_SMEM_LIMIT) {
+      smem += q;
+      flags |= 2;
+    }
+  }
   cudaError_t err = cudaFuncSetAttribute(k_eig<CPLX, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  PD_TIMED(ep.method == EIG_MODE_TOP1 ? "eig_mc" : "eig", s, k_eig<CPLX, NS><<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, in_smem ? 1 : 0));
+  PD_TIMED(ep.method == EIG_MODE_TOP1 ? "eig_mc" : "eig", s, k_eig<CPLX, NS><<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, flags));
   return cudaGetLastError();
 }
 

@@ -3,7 +3,9 @@
 // Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
 // as 1, 2, 3", SC'11) keyed by the 64-bit seed, counter (column group, row lo,
 // row hi, draw); the four output words give four normals by the Box-Muller
-// transform, so element (r, c) of draw d is a pure function of (seed, d, r, c).
+// transform (hardware-approximate log / sin / cos: their error is far below the
+// Monte-Carlo spread of the level), so element (r, c) of draw d is a pure
+// function of (seed, d, r, c).
 #pragma once
 #include <stdint.h>
 
@@ -35,9 +37,9 @@ __device__ __forceinline__ void normals4(uint64_t seed, uint32_t draw, uint64_t 
     // u1 in (0, 1], u2 in [0, 1)
     const float u1 = ((float)c[2 * h] + 1.0f) * 2.3283064365386963e-10f;
     const float u2 = (float)c[2 * h + 1] * 2.3283064365386963e-10f;
-    const float rad = sqrtf(-2.0f * logf(u1));
+    const float rad = sqrtf(-2.0f * __logf(u1));
     float sn, cs;
-    sincospif(2.0f * u2, &sn, &cs);
+    __sincosf(6.283185307179586f * u2, &sn, &cs);
     z[2 * h] = rad * cs;
     z[2 * h + 1] = rad * sn;
   }
