@@ -170,17 +170,59 @@ def reference_arm(args, rank, world):
 
 # --------------------------------------------------------------------------- GPU arm
 def algorithmic(kernel, n_patches, M, n, ranks):
-    """(algorithmic FLOPs or bytes per call, unit kind) of a library kernel for this workload."""
-    if kernel == "gram_fp32" or kernel == "gram_tc":
-        return 4.0 * M * n * (n + 1) * n_patches, "flop"  # complex Hermitian rank-M update, lower triangle
+    """(algorithmic work per call, "flop" or "byte") of a library kernel for this workload (complex64)."""
+    P = n_patches
+    if kernel in ("gram_fp32", "gram_tc"):
+        return 4.0 * M * n * (n + 1) * P, "flop"  # complex Hermitian rank-M update, lower triangle
     if kernel in ("mc_gram", "mc_gram_tc"):
-        rows = M * n
-        return float(N_ITER) * rows * n * (n + 1), "flop"
+        return float(N_ITER) * M * n * n * (n + 1), "flop"  # draws of (M n) x n, lower triangle
+    if kernel == "eig":
+        return 16.0 / 3.0 * n**3 * P, "flop"  # complex Householder tridiagonalisation
     if kernel == "synth_scatter":
         return float(np.sum(16.0 * M * n * ranks)), "flop"
-    if kernel == "eig":
-        return 16.0 / 3.0 * n**3 * n_patches, "flop"
+    if kernel == "gauss_pack":
+        return 2.0 * N_ITER * M * n * n, "byte"  # bf16 normals written
+    if kernel == "pack":
+        return 8.0 * M * n * P + 8.0 * M * n * P, "byte"  # complex rows in; bf16 hi and lo of the M x 2n real embedding out
+    if kernel == "patch_mean":
+        return 8.0 * M * n * P, "byte"
     return None, None
+
+
+# DRAM bytes per launch from the ncu captures summarised under profiles/
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch).
+NCU_TRAFFIC = {
+    "eig": 65.276e6 + 0.242e6,  # profiles/k_eig_c64_n200_405patches.md
+    "mc_gram_tc": 1.478e9 + 0.114e9,  # profiles/k_gram_tma_mc_draws_10x266200x200.md
+    "gauss_pack": 0.093e6 + 1.006e9,  # profiles/k_gauss_pack_10x266200x200.md
+}
+
+
+def roofline(name, per_launch_ms, launches, steps, work, kind, peaks):
+    """Achieved vs peak for one kernel: tensor kernels against the measured bf16 peak,
+    CUDA-core FP32 kernels against 148 SMs x 128 lanes x 2 FLOP x clock, memory-bound ones against HBM."""
+    per_launch = work * steps / launches
+    if kind == "byte":
+        achieved = per_launch / (per_launch_ms * 1e-3) / 1e9
+        peak = peaks.get("hbm_gbs", 6650.0)
+        bound, unit = "hbm", "GB/s"
+        src = "measured HBM copy (MEASURED_PEAKS.json)" if "hbm_gbs" in peaks else "fallback"
+    elif name in ("gram_tc", "mc_gram_tc"):
+        achieved = per_launch / (per_launch_ms * 1e-3) / 1e12
+        peak = peaks.get("bf16_tflops", 1590.0)
+        bound, unit = "tensor", "TFLOP/s"
+        src = "measured bf16 dense burst (MEASURED_PEAKS.json)" if "bf16_tflops" in peaks else "fallback"
+    else:
+        achieved = per_launch / (per_launch_ms * 1e-3) / 1e12
+        mhz = peaks.get("sm_max_mhz", 1965.0)
+        peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+        bound, unit = "fp32-simt", "TFLOP/s"
+        src = f"nominal FP32 CUDA-core peak, 148 SMs x 128 lanes x 2 FLOP x {mhz:.0f} MHz (no measured FP32 figure)"
+    tr = NCU_TRAFFIC.get(name)
+    return {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+            "frac": achieved / peak, "traffic": tr, "algorithmic_per_launch": per_launch,
+            "algorithmic_unit": "FLOP" if kind == "flop" else "byte", "peak_source": src,
+            "per_launch_ms": per_launch_ms, "launches": launches}
 
 
 def ours_arm(args, rank, world):
@@ -275,22 +317,20 @@ def ours_arm(args, rank, world):
         launches = int(sum(v[0] for v in kern.values())) // max(args.steps, 1)
         top = max(kern.items(), key=lambda kv: kv[1][1]) if kern else None
         roof = None
-        if top:
-            name, (nl, tot) = top
-            per_launch_ms = tot / nl
+        others = []
+        peaks = {}
+        pk_path = ROOT / "MEASURED_PEAKS.json"
+        if pk_path.exists():
+            peaks = json.loads(pk_path.read_text())
+        for name, (nl, tot) in sorted(kern.items(), key=lambda kv: -kv[1][1]):
             work, kind = algorithmic(name, n_p, M, n, ranks)
-            peaks = {}
-            pk_path = ROOT / "MEASURED_PEAKS.json"
-            if pk_path.exists():
-                peaks = json.loads(pk_path.read_text())
-            if kind == "flop":
-                per_launch = work * args.steps / nl
-                achieved = per_launch / (per_launch_ms * 1e-3) / 1e12
-                peak = peaks.get("bf16_tflops", 1590.0)
-                roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                        "frac": achieved / peak, "traffic": None,
-                        "peak_source": "measured bf16 dense (MEASURED_PEAKS.json)" if peaks else "fallback",
-                        "per_launch_ms": per_launch_ms, "launches": nl}
+            if work is None:
+                continue
+            r = roofline(name, tot / nl, nl, args.steps, work, kind, peaks)
+            if top and name == top[0]:
+                roof = r
+            else:
+                others.append(r)
         line = {
             "metric": METRIC, "value": world * vf / (ms * 1e-3), "unit": "voxel-frames/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -303,6 +343,7 @@ def ours_arm(args, rank, world):
             "e2e": {"value": world * vf / (e2e_ms * 1e-3), "unit": "voxel-frames/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
             "roofline": roof,
+            "rooflines_other": others,
             "kernels_ms_per_step": {k: v[1] / args.steps for k, v in kern.items()},
             "gpu_launches": launches,
             "clocks": clocks,
