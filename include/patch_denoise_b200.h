@@ -151,6 +151,25 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
                                  int32_t precision, double* out, void* d_workspace,
                                  size_t workspace_bytes, void* stream);
 
+/* NORDIC in one call, without a host round trip for the Monte-Carlo level.
+ * The reference computes the level on the host (space_time/lowrank.py:221-242)
+ * and then runs the patch loop with threshold = noise_std * level; this call
+ * does both on the device, in stream order: the draws (pd_nordic_mc_threshold's
+ * computation, with mc_rows x g->cols draws), the level, then the patch loop,
+ * whose eigensolver reads the threshold from device memory.
+ * p->method must be PD_METHOD_RAW; p->threshold is ignored.
+ *   d_level   2 doubles on the device: [0] the level, [1] noise_std * level
+ *   d_mc_ws   pd_nordic_workspace_size(mc_rows, g->cols, n_iter) bytes
+ * The other arguments are those of pd_denoise_patches (no noise map). Check
+ * both workspaces with pd_workspace_check. Replaces NordicDenoiser.denoise's level
+ * and patch loop (space_time/lowrank.py:221-246 and base.py:235-258). */
+pd_status pd_nordic_denoise_patches(const pd_geometry* g, const pd_params* p, double noise_std, int64_t mc_rows,
+                                    int32_t n_iter, uint64_t seed, double* d_level, void* d_mc_ws,
+                                    size_t mc_ws_bytes, const void* d_in, const int32_t* d_patch_list,
+                                    int64_t n_selected, void* d_out_acc, float* d_weight_acc, float* d_noise_acc,
+                                    float* d_noise_ctr, int32_t* d_rank_map, int32_t* d_patch_rank,
+                                    float* d_patch_noise, void* d_workspace, size_t workspace_bytes, void* stream);
+
 /* pd_denoise_patches without a workspace argument. No counterpart in the
  * reference. It is for callers that cannot allocate device memory while they
  * denoise, e.g. a host application that manages a fixed device-memory budget

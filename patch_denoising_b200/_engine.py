@@ -72,6 +72,7 @@ class DeviceResult:
     patch_index: torch.Tensor
     patch_rank: torch.Tensor
     patch_noise: torch.Tensor
+    level: torch.Tensor | None = None  # NORDIC: float64 [level, noise_std * level]
 
 
 def compute_dtype(dtype) -> torch.dtype:
@@ -154,11 +155,15 @@ def run(
     loss: str = "fro",
     mp_med: float = 0.0,
     precision: str = "fp32",
+    nordic: dict | None = None,
 ) -> DeviceResult:
     """Denoise ``data`` (device tensor, float32 or complex64, C-contiguous).
 
     ``mask``: uint8 device tensor of the data shape or of its spatial shape, or None.
     ``noise_std``: float64 device tensor of the spatial shape, or None.
+    ``nordic``: {"noise_std", "rows", "n_iter", "seed"}: compute the NORDIC
+    Monte-Carlo level on the device ahead of the patch loop, with no host
+    round trip (``pd_nordic_denoise_patches``); ``threshold`` is then unused.
     """
     lib = _lib.load()
     device = data.device
@@ -214,12 +219,27 @@ def run(
     pnoise = torch.zeros(max(n_sel, 1), dtype=torch.float32, device=device)
     _lib.check(lib.pd_denoise_workspace_size(gp, pp, n_sel, ctypes.byref(need)))
     ws = torch.empty(max(need.value, 1), dtype=torch.uint8, device=device)
-    _lib.check(
-        lib.pd_denoise_patches(
-            gp, pp, _vp(data), _vp(noise_std), _vp(plist), n_sel, _vp(out), _vp(wacc), _vp(nacc), _vp(nctr),
-            _vp(rank_map), _vp(prank), _vp(pnoise), _vp(ws), need.value, s,
+    level = mc_ws = None
+    if nordic is None:
+        _lib.check(
+            lib.pd_denoise_patches(
+                gp, pp, _vp(data), _vp(noise_std), _vp(plist), n_sel, _vp(out), _vp(wacc), _vp(nacc), _vp(nctr),
+                _vp(rank_map), _vp(prank), _vp(pnoise), _vp(ws), need.value, s,
+            )
         )
-    )
+    else:
+        mc_need = ctypes.c_size_t()
+        rows, n_iter = int(nordic["rows"]), int(nordic["n_iter"])
+        _lib.check(lib.pd_nordic_workspace_size(rows, int(g.cols), n_iter, ctypes.byref(mc_need)))
+        mc_ws = torch.empty(max(mc_need.value, 1), dtype=torch.uint8, device=device)
+        level = torch.empty(2, dtype=torch.float64, device=device)
+        _lib.check(
+            lib.pd_nordic_denoise_patches(
+                gp, pp, float(nordic["noise_std"]), rows, n_iter, ctypes.c_uint64(int(nordic["seed"]) & (2**64 - 1)),
+                _vp(level), _vp(mc_ws), mc_need.value, _vp(data), _vp(plist), n_sel, _vp(out), _vp(wacc),
+                _vp(nacc), _vp(nctr), _vp(rank_map), _vp(prank), _vp(pnoise), _vp(ws), need.value, s,
+            )
+        )
     weights = torch.empty(shape, dtype=torch.float32, device=device)
     noise_map = torch.empty(shape, dtype=torch.float32, device=device)
     _lib.check(
@@ -228,4 +248,6 @@ def run(
     )
     if n_sel:
         _lib.check(lib.pd_workspace_check(_vp(ws), s))
-    return DeviceResult(out, weights, noise_map, rank_map, plist[:n_sel], prank[:n_sel], pnoise[:n_sel])
+    if mc_ws is not None:
+        _lib.check(lib.pd_workspace_check(_vp(mc_ws), s))
+    return DeviceResult(out, weights, noise_map, rank_map, plist[:n_sel], prank[:n_sel], pnoise[:n_sel], level)

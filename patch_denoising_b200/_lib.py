@@ -76,6 +76,11 @@ SIGNATURES = {
     "pd_finalize": (c_i32, [G_P, P_P, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp]),
     "pd_nordic_workspace_size": (c_i32, [c_i64, c_i64, c_i32, ctypes.POINTER(c_sz)]),
     "pd_nordic_mc_threshold": (c_i32, [c_i64, c_i64, c_i32, ctypes.c_uint64, c_i32, ctypes.POINTER(c_dbl), c_vp, c_sz, c_vp]),
+    "pd_nordic_denoise_patches": (
+        c_i32,
+        [G_P, P_P, c_dbl, c_i64, c_i32, ctypes.c_uint64, c_vp, c_vp, c_sz, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp,
+         c_vp, c_vp, c_vp, c_vp, c_vp, c_sz, c_vp],
+    ),
     "pd_denoise_patches_noalloc": (
         c_i32,
         [G_P, P_P, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],

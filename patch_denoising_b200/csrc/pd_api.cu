@@ -96,15 +96,6 @@ PatchWork carve_work(void* ws, int count, int n, bool cplx, size_t* used, size_t
   return w;
 }
 
-int64_t tc_rows_per_cta(int64_t rows) {
-  int64_t r = (rows + 147) / 148;
-  return (r + 63) & ~int64_t(63);
-}
-int64_t tc_chunks(int64_t rows) {
-  const int64_t r = tc_rows_per_cta(rows);
-  return (rows + r - 1) / r;
-}
-
 size_t work_bytes(int count, int n, bool cplx, size_t packed_per_patch = 0) {
   size_t used;
   carve_work(nullptr, count, n, cplx, &used, packed_per_patch);
@@ -331,11 +322,13 @@ pd_status pd_denoise_workspace_size(const pd_geometry* g, const pd_params* p, in
   return PD_OK;
 }
 
-pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const void* d_in, const double* d_noise_std,
-                             const int32_t* d_patch_list, int64_t n_selected, void* d_out_acc, float* d_weight_acc,
-                             float* d_noise_acc, float* d_noise_ctr, int32_t* d_rank_map, int32_t* d_patch_rank,
-                             float* d_patch_noise, void* d_ws, size_t ws_bytes, void* stream) {
-  g_err.clear();
+// pd_denoise_patches with the raw threshold optionally read on the device
+// (d_thr; NULL = p->threshold), for the one-call NORDIC path.
+static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, const void* d_in,
+                                      const double* d_noise_std, const int32_t* d_patch_list, int64_t n_selected,
+                                      void* d_out_acc, float* d_weight_acc, float* d_noise_acc, float* d_noise_ctr,
+                                      int32_t* d_rank_map, int32_t* d_patch_rank, float* d_patch_noise, void* d_ws,
+                                      size_t ws_bytes, void* stream, const double* d_thr) {
   PD_TRY(check_geometry(g));
   PD_TRY(check_params(g, p));
   if (n_selected == 0) return PD_OK;
@@ -364,6 +357,7 @@ pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const voi
   ep.threshold_scale = p->threshold_scale;
   ep.threshold = p->threshold;
   ep.mp_median = p->mp_median;
+  ep.d_threshold = d_thr;
   PD_TRY(cuda_check(cudaMemsetAsync(d_ws, 0, sizeof(int), s), "clear error word"));
   for (int64_t off = 0; off < n_selected; off += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_selected - off);
@@ -394,6 +388,15 @@ pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const voi
   return PD_OK;
 }
 
+pd_status pd_denoise_patches(const pd_geometry* g, const pd_params* p, const void* d_in, const double* d_noise_std,
+                             const int32_t* d_patch_list, int64_t n_selected, void* d_out_acc, float* d_weight_acc,
+                             float* d_noise_acc, float* d_noise_ctr, int32_t* d_rank_map, int32_t* d_patch_rank,
+                             float* d_patch_noise, void* d_ws, size_t ws_bytes, void* stream) {
+  g_err.clear();
+  return denoise_patches_impl(g, p, d_in, d_noise_std, d_patch_list, n_selected, d_out_acc, d_weight_acc, d_noise_acc,
+                              d_noise_ctr, d_rank_map, d_patch_rank, d_patch_noise, d_ws, ws_bytes, stream, nullptr);
+}
+
 pd_status pd_finalize(const pd_geometry* g, const pd_params* p, void* d_out, const float* d_weight_acc,
                       const float* d_noise_acc, const float* d_noise_ctr, float* d_weights, float* d_noise_map,
                       const uint8_t* d_mask, int32_t mask_is_4d, void* stream) {
@@ -419,15 +422,14 @@ pd_status pd_nordic_workspace_size(int64_t rows, int64_t cols, int32_t n_iter, s
   return PD_OK;
 }
 
-pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uint64_t seed, int32_t precision,
-                                 double* out, void* d_ws, size_t ws_bytes, void* stream) {
-  g_err.clear();
-  if (!out) return fail(PD_ERR_INVALID, "NULL output");
+// Launches the Monte-Carlo draws, their Grams and the top-1 eigenvalues on s
+// (eigenvalues to w.prior[0..n_iter)); no host synchronisation.
+static pd_status mc_launch(int64_t rows, int64_t cols, int32_t n_iter, uint64_t seed, int32_t precision, void* d_ws,
+                           size_t ws_bytes, cudaStream_t s, PatchWork* out) {
   size_t need;
   PD_TRY(pd_nordic_workspace_size(rows, cols, n_iter, &need));
   if (!d_ws || ws_bytes < need) return fail(PD_ERR_WORKSPACE, "workspace too small (%zu < %zu)", ws_bytes, need);
-  (void)precision;
-  cudaStream_t s = (cudaStream_t)stream;
+  if (n_iter > 4096) return fail(PD_ERR_UNSUPPORTED, "at most 4096 Monte-Carlo draws");
   const int n = (int)cols;
   size_t used;
   PatchWork w = carve_work(d_ws, n_iter, n, false, &used);
@@ -449,8 +451,18 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
   ep.rows = (int)std::min<int64_t>(rows, INT32_MAX);
   ep.cols = n;
   PD_TRY(cuda_check(launch_eig(false, n, ep, w, s), "Monte-Carlo eigensolver launch"));
+  *out = w;
+  return PD_OK;
+}
+
+pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uint64_t seed, int32_t precision,
+                                 double* out, void* d_ws, size_t ws_bytes, void* stream) {
+  g_err.clear();
+  if (!out) return fail(PD_ERR_INVALID, "NULL output");
+  cudaStream_t s = (cudaStream_t)stream;
+  PatchWork w;
+  PD_TRY(mc_launch(rows, cols, n_iter, seed, precision, d_ws, ws_bytes, s, &w));
   double lam[4096];
-  if (n_iter > 4096) return fail(PD_ERR_UNSUPPORTED, "at most 4096 Monte-Carlo draws");
   PD_TRY(cuda_check(cudaMemcpyAsync(lam, w.prior, sizeof(double) * n_iter, cudaMemcpyDeviceToHost, s), "copy"));
   PD_TRY(cuda_check(cudaStreamSynchronize(s), "Monte-Carlo sync"));
   int err = 0;
@@ -460,6 +472,29 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
   for (int i = 0; i < n_iter; ++i) acc += sqrt(fmax(lam[i], 0.0));
   *out = acc / n_iter;
   return PD_OK;
+}
+
+pd_status pd_nordic_denoise_patches(const pd_geometry* g, const pd_params* p, double noise_std, int64_t mc_rows,
+                                    int32_t n_iter, uint64_t seed, double* d_level, void* d_mc_ws, size_t mc_ws_bytes,
+                                    const void* d_in, const int32_t* d_patch_list, int64_t n_selected,
+                                    void* d_out_acc, float* d_weight_acc, float* d_noise_acc, float* d_noise_ctr,
+                                    int32_t* d_rank_map, int32_t* d_patch_rank, float* d_patch_noise, void* d_ws,
+                                    size_t ws_bytes, void* stream) {
+  g_err.clear();
+  PD_TRY(check_geometry(g));
+  PD_TRY(check_params(g, p));
+  if (p->method != PD_METHOD_RAW) return fail(PD_ERR_INVALID, "pd_nordic_denoise_patches needs method RAW");
+  if (!d_level) return fail(PD_ERR_INVALID, "NULL level output");
+  cudaStream_t s = (cudaStream_t)stream;
+  // the draws, their Grams and top-1 eigenvalues, then the level and the threshold on the device
+  PatchWork mw;
+  PD_TRY(mc_launch(mc_rows, g->cols, n_iter, seed, p->precision, d_mc_ws, mc_ws_bytes, s, &mw));
+  launch_mc_level(mw.prior, n_iter, noise_std, d_level, s);
+  PD_TRY(cuda_check(cudaGetLastError(), "Monte-Carlo level launch"));
+  // the patch loop reads the threshold from d_level[1]
+  return denoise_patches_impl(g, p, d_in, nullptr, d_patch_list, n_selected, d_out_acc, d_weight_acc, d_noise_acc,
+                              d_noise_ctr, d_rank_map, d_patch_rank, d_patch_noise, d_ws, ws_bytes, stream,
+                              d_level + 1);
 }
 
 pd_status pd_workspace_check(const void* d_workspace, void* stream) {

@@ -122,17 +122,22 @@ __device__ __forceinline__ float warp_min(float v) {
 // v_j(j+1) = 1, and updates the trailing block A22 <- A22 - v w^H - w v^H with
 // p = A22 v, w = tau p + alpha v, alpha = -tau/2 (tau p)^H v.
 //
-// Three block barriers per step. The rank-2 update of step j-1 and the product
+// Four block barriers per step. The rank-2 update of step j-1 and the product
 // p_j = A22 v_j of step j share one pass over A22, so each stored element is
 // loaded, updated, stored and multiplied once per step; only column j, which
-// reflector j is built from, takes its update ahead of the pass (warp 0).
-//   phase 1 (warp 0): alpha_{j-1}; column j -= update_{j-1}; reflector j
+// reflector j is built from, takes its update ahead of the pass.
+//   phase 1 (all):    alpha_{j-1} (each warp, from the per-warp partials);
+//                     column j -= update_{j-1}, a thread per row; its norm
+//                     (barrier); reflector j, its scalars formed by every
+//                     thread                                    (barrier)
 //   phase 2 (all):    A22 -= update_{j-1}; partial sums of A22 v_j: warps own
 //                     columns k, lanes own rows i = lane + 32 s (registers); the
 //                     row part A22(i,k) v_k accumulates in registers, the
 //                     transposed part sum_i conj(A22(i,k)) v_i is reduced over
 //                     lanes eight columns at a time (reduce-scatter butterfly)
+//                                                               (barrier)
 //   phase 3 (all):    p_j from the partials; tau_j p_j; partials of (tau p)^H v
+//                                                               (barrier)
 // v and tau p live in two buffers of n entries indexed by row (step parity).
 // ---------------------------------------------------------------------------
 template <class T>
@@ -186,9 +191,9 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
                                typename Elem<CPLX>::T* pw, typename Elem<CPLX>::T* pd) {
   using T = typename Elem<CPLX>::T;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  __shared__ T s_red[EIG_NW];  // per-warp partials of (tau p)^H v
-  __shared__ T s_alpha;        // alpha of the previous step
-  __shared__ T s_tau;          // tau of the current step
+  __shared__ T s_red[EIG_NW];     // per-warp partials of (tau p)^H v
+  __shared__ float s_x2[EIG_NW];  // per-warp partials of the column norm
+  __shared__ T s_sub;             // A(j+1, j) after its last update
   T one;
   if constexpr (CPLX) one = cf{1.f, 0.f};
   else one = 1.f;
@@ -198,7 +203,7 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
     wb[i] = zero<T>();
   }
   if (tid < EIG_NW) s_red[tid] = zero<T>();
-  T tau_prev = zero<T>();  // warp 0: tau of the previous step
+  T tau_prev = zero<T>();  // tau of the previous step (every thread)
   __syncthreads();
   for (int j = 0; j < n - 1; ++j) {
     const int m = n - j - 1;
@@ -207,36 +212,38 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
     T* wc = wb + cur * n;
     const T* vp = vb + (cur ^ 1) * n;
     const T* wp = wb + (cur ^ 1) * n;
-    // ---- phase 1 (warp 0): finish column j, build reflector j
-    if (warp == 0) {
+    // ---- phase 1 (all): finish column j (thread t owns row j + t), build reflector j
+    T al, tj = zero<T>();
+    {
       T dot = lane < EIG_NW ? s_red[lane] : zero<T>();
       dot = warp_sum(dot);
-      const T al = mul(tau_prev, dot) * -0.5f;  // w_{j-1} = tau p + al v
-      const T vj = vp[j];
-      const T cuj = cj(wp[j] + mul(al, vj)), cvj = cj(vj);
-      T col[NS];
-      float xn2 = 0.f;
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        const int r = j + lane + 32 * s;
-        col[s] = zero<T>();
-        if (r < n) {
-          const T v = vp[r];
-          const T u = wp[r] + mul(al, v);
-          const T a = A[pk(r, j, n)] - (mul(v, cuj) + mul(u, cvj));
-          col[s] = a;
-          if (r >= j + 2) xn2 += abs2(a);
-        }
+      al = mul(tau_prev, dot) * -0.5f;  // w_{j-1} = tau p + al v
+      const int r = j + tid;            // n - j <= n <= EIG_THREADS rows
+      T a = zero<T>();
+      float x2 = 0.f;
+      if (r < n) {
+        const T vj = vp[j];
+        const T cuj = cj(wp[j] + mul(al, vj)), cvj = cj(vj);
+        const T v = vp[r];
+        const T u = wp[r] + mul(al, v);
+        a = A[pk(r, j, n)] - (mul(v, cuj) + mul(u, cvj));
+        if (r >= j + 2) x2 = abs2(a);
       }
+      x2 = warp_sum(x2);
+      if (lane == 0) s_x2[warp] = x2;
+      if (tid == 1) s_sub = a;  // A(j+1, j)
+      if (tid == 0) d[j] = re(a);
+      __syncthreads();
+      float xn2 = lane < EIG_NW ? s_x2[lane] : 0.f;
       xn2 = warp_sum(xn2);
-      const T alpha = shfl_idx(col[0], 1);  // A(j+1, j)
+      const T alpha = s_sub;
       const float ar = re(alpha);
       float ai = 0.f;
       if constexpr (CPLX) ai = alpha.y;
       const bool refl = !(xn2 == 0.f && ai == 0.f);
-      T tj = zero<T>(), inv = zero<T>();
+      T inv = zero<T>();
       float ej = ar;
-      if (refl) {
+      if (refl) {  // every thread forms the same scalars
         const float nrm = sqrtf(ar * ar + ai * ai + xn2);
         const float beta = ar >= 0.f ? -nrm : nrm;
         if constexpr (CPLX) {
@@ -250,31 +257,23 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
         }
         ej = beta;
       }
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        const int r = j + lane + 32 * s;
-        if (r > j && r < n) {
-          T v = zero<T>();
-          if (refl) {
-            v = (r == j + 1) ? one : mul(col[s], inv);
-            if (r > j + 1) A[pk(r, j, n)] = v;
-          }
-          vc[r] = v;
+      if (r > j && r < n) {
+        T v = zero<T>();
+        if (refl) {
+          v = (r == j + 1) ? one : mul(a, inv);
+          if (r > j + 1) A[pk(r, j, n)] = v;
         }
+        vc[r] = v;
       }
-      if (lane == 0) {
-        d[j] = re(col[0]);
+      if (tid == 0) {
         e[j] = ej;
         tau[j] = tj;
-        s_tau = tj;
-        s_alpha = al;
       }
       tau_prev = tj;
     }
     __syncthreads();
     // ---- phase 2 (all): A22 -= update_{j-1}; partial sums of p = A22 v_j
     {
-      const T al = s_alpha;
       T vo[NS], uo[NS], vn[NS], acc[NS];
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
@@ -330,7 +329,6 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
     __syncthreads();
     // ---- phase 3 (all): w = tau p, partials of w^H v
     {
-      const T tj = s_tau;
       T dpart = zero<T>();
       if (tid < m) {
         const int r = j + 1 + tid;
@@ -428,7 +426,10 @@ __device__ void cta_eigs(const float* d, const float* e2, int n, const TriInfo& 
 constexpr int LANCZOS_STEPS = 48;
 
 // Q: (min(n, LANCZOS_STEPS) + 1) * n floats of scratch; al, be, be2: n floats each.
-__device__ float lanczos_top1(const float* A, int n, float* Q, float* al, float* be, float* be2) {
+// FULL = false: A is packed lower (ld unused); true: a full row-major square
+// with leading dimension ld (odd, so a thread per row reads conflict-free).
+template <bool FULL>
+__device__ float lanczos_top1(const float* A, int n, int ld, float* Q, float* al, float* be, float* be2) {
   __shared__ float s_coef[LANCZOS_STEPS];
   __shared__ float s_val;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -450,12 +451,27 @@ __device__ float lanczos_top1(const float* A, int n, float* Q, float* al, float*
   int kk = kmax;
   for (int j = 0; j < kmax; ++j) {
     const float* qj = Q + (int64_t)j * n;
-    // w = A q_j: a warp per row, lanes over the columns
-    for (int r = warp; r < n; r += EIG_NW) {
-      float s = 0.f;
-      for (int k = lane; k < n; k += 32) s += A[k <= r ? pk(r, k, n) : pk(k, r, n)] * qj[k];
-      s = warp_sum(s);
-      if (lane == 0) wv[r] = s;
+    if constexpr (FULL) {
+      // w = A q_j: a thread per row
+      for (int r = tid; r < n; r += EIG_THREADS) {
+        const float* row = A + (int64_t)r * ld;
+        float s0 = 0.f, s1 = 0.f;
+        int k = 0;
+        for (; k + 1 < n; k += 2) {
+          s0 += row[k] * qj[k];
+          s1 += row[k + 1] * qj[k + 1];
+        }
+        if (k < n) s0 += row[k] * qj[k];
+        wv[r] = s0 + s1;
+      }
+    } else {
+      // w = A q_j: a warp per row, lanes over the columns
+      for (int r = warp; r < n; r += EIG_NW) {
+        float s = 0.f;
+        for (int k = lane; k < n; k += 32) s += A[k <= r ? pk(r, k, n) : pk(k, r, n)] * qj[k];
+        s = warp_sum(s);
+        if (lane == 0) wv[r] = s;
+      }
     }
     __syncthreads();
     float b2p = 0.f;
@@ -572,6 +588,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
   __shared__ int s_cnt, s_act, s_c0, s_c1;
   __shared__ double s_scale_true;  // 1/sc: true eigenvalue = scaled * this
   __shared__ double s_x0;
+  __shared__ double s_thr;  // raw / NORDIC threshold on singular values
 
   const int64_t np = pk_size(n);
   if (in_smem & 1) {
@@ -591,7 +608,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
   if constexpr (!CPLX) {
     if (ep.method == EIG_MODE_TOP1) {  // Monte-Carlo level: top eigenvalue only
       float* Q = (in_smem & 2) ? reinterpret_cast<float*>(sm + L.total) : w.vec + (int64_t)p * w.vec_stride;
-      const float lam1 = lanczos_top1(A, n, Q, d, e, e2);
+      const float lam1 = lanczos_top1<false>(A, n, 0, Q, d, e, e2);
       if (tid == 0) {
         w.prior[p] = (double)lam1 * s_scale_true;
         w.n_active[p] = 0;
@@ -690,7 +707,8 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
     __syncthreads();
   } else if (ep.method == PD_METHOD_RAW) {
     if (tid == 0) {
-      const double x = ep.threshold * ep.threshold / tscale;  // scaled threshold on eigenvalues
+      s_thr = ep.d_threshold ? *ep.d_threshold : ep.threshold;
+      const double x = s_thr * s_thr / tscale;  // scaled threshold on eigenvalues
       s_c0 = sturm_count(d, e2, n, (float)(x * (1.0 - CAND_MARGIN)), ti.pivmin);
     }
     __syncthreads();
@@ -702,7 +720,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
       int r = 0;
       for (int i = nc - 1; i >= 0; --i) {
         const double s = sqrt(fmax((double)lam[i] * tscale, 0.0));
-        if (s > ep.threshold) {
+        if (s > s_thr) {
           aidx[r] = idx[i];
           alam[r] = lam[i];
           acoef[r] = 1.f;
@@ -951,6 +969,50 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
   if (tid == 0) w.n_active[p] = act;
 }
 
+// Top-1 eigenvalue of each real packed Gram (the NORDIC Monte-Carlo draws),
+// the matrix scaled by its largest diagonal entry and expanded to a full square
+// with odd leading dimension in shared memory, so the Lanczos product is a
+// plain row-times-vector per thread. One CTA per draw.
+__host__ __device__ inline int top1_ld(int n) { return n | 1; }
+size_t top1_smem_bytes(int n) {
+  const int kmax = n < LANCZOS_STEPS ? n : LANCZOS_STEPS;
+  return sizeof(float) * ((size_t)n * top1_ld(n) + (size_t)(kmax + 1) * n + 3 * (size_t)n);
+}
+
+__global__ void __launch_bounds__(EIG_THREADS, 1) k_top1(int n, PatchWork w) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int p = blockIdx.x;
+  const int ld = top1_ld(n);
+  const int kmax = n < LANCZOS_STEPS ? n : LANCZOS_STEPS;
+  float* F = reinterpret_cast<float*>(sm);
+  float* Q = F + (size_t)n * ld;
+  float* al = Q + (size_t)(kmax + 1) * n;
+  float* be = al + n;
+  float* be2 = be + n;
+  __shared__ double s_md;
+  const float* G = w.gram + (int64_t)p * w.gram_stride;
+  float md = 0.f;
+  for (int i = tid; i < n; i += EIG_THREADS) md = fmaxf(md, G[pk(i, i, n)]);
+  md = bmax_f(md);
+  const float sc = md > 0.f ? 1.f / md : 1.f;
+  if (tid == 0) s_md = md > 0.f ? (double)md : 1.0;
+  for (int j = warp; j < n; j += EIG_NW) {
+    const int64_t cb = pk(j, j, n) - j;
+    for (int i = j + lane; i < n; i += 32) {
+      const float v = G[cb + i] * sc;
+      F[(size_t)i * ld + j] = v;
+      F[(size_t)j * ld + i] = v;
+    }
+  }
+  __syncthreads();
+  const float lam = lanczos_top1<true>(F, n, ld, Q, al, be, be2);
+  if (tid == 0) {
+    w.prior[p] = (double)lam * s_md;
+    w.n_active[p] = 0;
+  }
+}
+
 template <bool CPLX, int NS>
 static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
   bool in_smem;
@@ -979,6 +1041,15 @@ static cudaError_t eig_dispatch(int n, const EigParams& ep, const PatchWork& w, 
 }
 
 cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
+  if (!cplx && ep.method == EIG_MODE_TOP1) {
+    const size_t smem = top1_smem_bytes(n);
+    if (smem <= EIG_SMEM_LIMIT) {
+      cudaError_t err = cudaFuncSetAttribute(k_top1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (err != cudaSuccess) return err;
+      PD_TIMED("eig_mc", s, k_top1<<<w.count, EIG_THREADS, smem, s>>>(n, w));
+      return cudaGetLastError();
+    }
+  }
   return cplx ? eig_dispatch<true>(n, ep, w, s) : eig_dispatch<false>(n, ep, w, s);
 }
 

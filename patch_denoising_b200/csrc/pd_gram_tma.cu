@@ -90,32 +90,25 @@ __global__ void __launch_bounds__(256) k_pack_patches(Geo g, const float* __rest
 }
 
 // Gaussian draws, packed transposed: G^T[d][c][r] for r < rows (zero to kp).
-// grid: (kp / 64, ceil(cols / 64), draws), 256 threads.
+// A thread makes the normals of two consecutive rows and one group of four
+// columns (two Philox blocks) and stores them as bf16 pairs straight into the
+// four K-major column rows: a warp covers 64 consecutive rows, so every store
+// instruction writes 128 contiguous bytes, with no shared-memory transpose.
+// grid: (kp / 64, ceil(cols / 32), draws), 256 threads = 8 column groups.
 __global__ void __launch_bounds__(256) k_gauss_pack(int64_t rows, int cols, uint64_t seed,
                                                     __nv_bfloat16* __restrict__ out, int64_t kp) {
-  __shared__ float tile[PK_R][PK_C + 1];
-  const int64_t r0 = (int64_t)blockIdx.x * PK_R;
-  const int c0 = blockIdx.y * PK_C;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t r = (int64_t)blockIdx.x * PK_R + 2 * lane;
+  const int cg = blockIdx.y * 8 + warp;  // columns 4 cg .. 4 cg + 3
   const int d = blockIdx.z;
-  const int tid = threadIdx.x;
-  // 64 rows x 16 column groups of 4 = 1024 Philox blocks, 4 per thread
-  for (int t = tid; t < PK_R * (PK_C / 4); t += 256) {
-    const int rr = t / (PK_C / 4), cg = t % (PK_C / 4);
-    const int64_t r = r0 + rr;
-    const int col = c0 + cg * 4;
-    float z[4] = {0.f, 0.f, 0.f, 0.f};
-    if (r < rows && col < cols) normals4(seed, (uint32_t)d, (uint64_t)r, (uint32_t)(col >> 2), z);
+  if (4 * cg >= cols) return;
+  float z0[4] = {0.f, 0.f, 0.f, 0.f}, z1[4] = {0.f, 0.f, 0.f, 0.f};
+  if (r < rows) normals4(seed, (uint32_t)d, (uint64_t)r, (uint32_t)cg, z0);
+  if (r + 1 < rows) normals4(seed, (uint32_t)d, (uint64_t)(r + 1), (uint32_t)cg, z1);
+  __nv_bfloat16* op = out + ((int64_t)d * cols + 4 * cg) * kp + r;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) tile[rr][cg * 4 + q] = (col + q < cols) ? z[q] : 0.f;
-  }
-  __syncthreads();
-  const int warp = tid >> 5, lane = tid & 31;
-  __nv_bfloat16* op = out + (int64_t)d * cols * kp;
-  for (int cc = warp; cc < PK_C; cc += 8) {
-    const int colw = c0 + cc;
-    if (colw >= cols) break;
-    pack_store(op, nullptr, (int64_t)colw * kp + r0 + 2 * lane, tile[2 * lane][cc], tile[2 * lane + 1][cc]);
-  }
+  for (int q = 0; q < 4; ++q)
+    if (4 * cg + q < cols) *reinterpret_cast<__nv_bfloat162*>(op + (int64_t)q * kp) = __floats2bfloat162_rn(z0[q], z1[q]);
 }
 
 // ---------------------------------------------------------------------------
@@ -398,7 +391,7 @@ cudaError_t launch_gauss_gram_packed(int64_t rows, int cols, int n_iter, uint64_
                                      int64_t part_stride, int* err, cudaStream_t s) {
   const int64_t kp = pack_k(rows);
   __nv_bfloat16* g = reinterpret_cast<__nv_bfloat16*>(packed);
-  dim3 pg((unsigned)(kp / PK_R), (cols + PK_C - 1) / PK_C, n_iter);
+  dim3 pg((unsigned)(kp / PK_R), (cols + 31) / 32, n_iter);
   PD_TIMED("gauss_pack", s, k_gauss_pack<<<pg, 256, 0, s>>>(rows, cols, seed, g, kp));
   CUtensorMap mh;
   cudaError_t e = make_map(&mh, g, kp, cols, n_iter);

@@ -58,6 +58,7 @@ struct EigParams {
   double threshold_scale;
   double threshold;
   double mp_median;
+  const double* d_threshold;  // raw / NORDIC: read the threshold here when not NULL
 };
 constexpr int EIG_MODE_TOP1 = 100;
 cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s);
@@ -95,6 +96,7 @@ int64_t mc_chunks(int64_t rows);
 void launch_gauss_fill(int64_t rows, int cols, uint64_t seed, int draw, float* out, cudaStream_t s);
 void launch_chunk_reduce(const float* part, int64_t part_stride, int chunks, int64_t np, int draws, float* gram,
                          int64_t gram_stride, cudaStream_t s);
+void launch_mc_level(const double* lam, int n_iter, double noise_std, double* out, cudaStream_t s);
 void launch_mc_gram(int64_t rows, int cols, int n_iter, uint64_t seed, float* part, float* gram,
                     int64_t gram_stride, cudaStream_t s);
 

@@ -129,6 +129,22 @@ void launch_chunk_reduce(const float* part, int64_t part_stride, int chunks, int
   PD_TIMED("mc_reduce", s, k_mc_reduce<<<rgrid, 256, 0, s>>>(part, part_stride, chunks, np, gram, gram_stride));
 }
 
+// level = mean_i sqrt(max(lam_i, 0)) in draw order (the host formula of
+// pd_nordic_mc_threshold, so both give the same double); out = {level, noise_std * level}.
+__global__ void k_mc_level(const double* __restrict__ lam, int n_iter, double noise_std, double* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double acc = 0.0;
+    for (int i = 0; i < n_iter; ++i) acc += sqrt(fmax(lam[i], 0.0));
+    const double level = acc / n_iter;
+    out[0] = level;
+    out[1] = noise_std * level;
+  }
+}
+
+void launch_mc_level(const double* lam, int n_iter, double noise_std, double* out, cudaStream_t s) {
+  PD_TIMED("mc_level", s, k_mc_level<<<1, 32, 0, s>>>(lam, n_iter, noise_std, out));
+}
+
 void launch_mc_gram(int64_t rows, int cols, int n_iter, uint64_t seed, float* part, float* gram,
                     int64_t gram_stride, cudaStream_t s) {
   const int nt = (cols + MC_T - 1) / MC_T;

@@ -121,6 +121,9 @@ class BaseSpaceTimeDenoiser(abc.ABC):
         """Per-method arguments of ``_engine.run`` (overridden by subclasses)."""
         return {}
 
+    def _take_result(self, res):
+        """Hook for subclasses that keep more of the device result."""
+
     def _denoise(self, input_data, mask, mask_threshold, progbar):
         if not torch.cuda.is_available():
             raise RuntimeError("patch_denoising_b200 needs a CUDA device (sm_100a); no CPU fallback exists")
@@ -141,6 +144,7 @@ class BaseSpaceTimeDenoiser(abc.ABC):
         self.patch_index_ = res.patch_index
         self.patch_rank_ = res.patch_rank
         self.patch_noise_ = res.patch_noise
+        self._take_result(res)
         if progbar is not None and progbar is not False:
             progbar.reset(total=int(res.patch_index.numel()))
             progbar.update(int(res.patch_index.numel()))

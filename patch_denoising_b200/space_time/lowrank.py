@@ -68,7 +68,9 @@ class NordicDenoiser(RawSVDDenoiser):
     standard Gaussian draws ``G_n`` of ``prod(patch_shape incl. time) x T``,
     computed on the GPU (counter-based generator seeded from NumPy's global
     generator, so ``np.random.seed`` makes a call reproducible, as in the
-    reference). ``mc_max_sval`` (extension) supplies that mean directly.
+    reference). The threshold never leaves the device (no host round trip in
+    the call); ``mc_max_sval_`` reads the level back on first access. ``mc_max_sval`` (extension) supplies the
+    level directly.
     """
 
     _method = "nordic"
@@ -85,17 +87,31 @@ class NordicDenoiser(RawSVDDenoiser):
             )
         shape = tuple(input_data.shape)
         patch_shape, _ = self._get_patch_param(shape)
+        self._nordic = None
+        self._level = None
         if mc_max_sval is None:
-            import torch
-
             seed = int(np.random.randint(0, 2**62))
-            device = input_data.device if isinstance(input_data, torch.Tensor) and input_data.is_cuda else \
-                torch.device("cuda", torch.cuda.current_device())
-            mc_max_sval = _engine.nordic_max_sval(int(np.prod(patch_shape)), shape[-1], n_iter_threshold, seed,
-                                                  device, self.precision)
-        self.mc_max_sval_ = float(mc_max_sval)
-        self._threshold = float(noise_std) * float(mc_max_sval)
+            self._nordic = {"noise_std": float(noise_std), "rows": int(np.prod(patch_shape)),
+                            "n_iter": int(n_iter_threshold), "seed": seed}
+            self._threshold = 0.0
+            self._mc_max_sval = None
+        else:
+            self._mc_max_sval = float(mc_max_sval)
+            self._threshold = float(noise_std) * float(mc_max_sval)
         return self._denoise(input_data, mask, mask_threshold, progbar)
+
+    @property
+    def mc_max_sval_(self):
+        """Mean largest singular value of the Monte-Carlo draws of the last call."""
+        if self._mc_max_sval is None and self._level is not None:
+            self._mc_max_sval = float(self._level[0].item())
+        return self._mc_max_sval
+
+    def _method_args(self, data_shape, p_s, device):
+        return {"threshold": float(self._threshold), "nordic": self._nordic}
+
+    def _take_result(self, res):
+        self._level = res.level
 
 
 class OptimalSVDDenoiser(BaseSpaceTimeDenoiser):

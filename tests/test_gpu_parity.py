@@ -85,6 +85,30 @@ def test_nordic_monte_carlo_level_statistics():
     assert again == ours
 
 
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_nordic_level_on_device_matches_host_level(precision):
+    """The one-call NORDIC path (level and threshold kept on the device) gives the
+    host-computed level bit for bit, and the same output as the two-step path
+    given that level."""
+    from patch_denoising_b200 import NordicDenoiser
+
+    x, _ = lowrank_volume((22, 22, 12, 48), 4, seed=12, complex_valued=True)
+    np.random.seed(5)
+    den = NordicDenoiser(7, 3, precision=precision)
+    out1, w1, _, rm1 = den.denoise(x, noise_std=1.0, n_iter_threshold=4)
+    np.random.seed(5)
+    seed = int(np.random.randint(0, 2**62))
+    host = _engine.nordic_max_sval(7**3 * 48, 48, 4, seed, torch.device("cuda", 0), precision)
+    assert den.mc_max_sval_ == host
+    out2, w2, _, rm2 = NordicDenoiser(7, 3, precision=precision).denoise(x, noise_std=1.0, mc_max_sval=host)
+    np.testing.assert_array_equal(np.isnan(out1), np.isnan(out2))
+    np.testing.assert_array_equal(rm1, rm2)  # same threshold, same decisions
+    fin = ~np.isnan(out1)
+    # the scatter adds in atomic order, so equal up to float32 summation order
+    assert rel_l2(out1[fin].astype(np.complex128), out2[fin].astype(np.complex128)) <= 1e-6
+    assert rel_l2(w1.astype(np.float64), w2.astype(np.float64)) <= 1e-6
+
+
 def test_torch_input_stays_on_device():
     x, _ = lowrank_volume((20, 20, 12, 40), 3, seed=8)
     xt = torch.from_numpy(x).cuda()
