@@ -10,9 +10,12 @@ from .oracle import (  # noqa: F401
     denoise,
     eig_analysis,
     eig_synthesis,
+    estimate_noise,
+    estimate_noise_covered,
     grid_geometry,
     marchenko_pastur_median,
     nordic_threshold,
+    patch_locs,
     patch_params,
     select_patches,
     svd_analysis,

@@ -497,3 +497,60 @@ def denoise(
         "threshold": thr,
         "mp_median": mp_med,
     }
+
+
+# --------------------------------------------------------------------------- #
+# Noise map from a noise-only sequence                                        #
+# --------------------------------------------------------------------------- #
+def patch_locs(p_shape, p_ovl, v_shape):
+    """Top-left corners of all patches (space_time/utils.py:8-55, ``get_patch_locs``).
+
+    Per axis: ``arange(0, v - p, p - o)`` plus the last index ``v - p`` when the
+    range stops short of it; an axis with ``v <= p`` gives an empty range, on
+    which the reference's ``range_[-1]`` raises IndexError, as here.
+    """
+    if len(v_shape) != len(p_shape) or len(v_shape) != len(p_ovl):
+        raise ValueError(f"Dimension mismatch between the arguments. {p_shape}{p_ovl}, {v_shape}")
+    ranges = []
+    for v_s, p_s, p_o in zip(v_shape, p_shape, p_ovl):
+        if p_o >= p_s:
+            raise ValueError("Overlap should be a non-negative integer smaller than patch_size")
+        last = v_s - p_s
+        r = np.arange(0, last, p_s - p_o, dtype=np.int32)
+        if r[-1] < last:  # IndexError on an empty range, as in the reference
+            r = np.append(r, last)
+        ranges.append(r)
+    grids = np.meshgrid(*ranges, indexing="ij")
+    return np.stack([g.reshape(-1) for g in grids], axis=1)
+
+
+def estimate_noise(noise_sequence, block_size=1):
+    """Noise map of a noise-only sequence (space_time/utils.py:207-242).
+
+    For every block of ``block_size`` voxels per spatial axis (overlap
+    ``block_size - 1``: every position), the voxel at the block's centre
+    (top-left + ``block_size // 2``) gets the population standard deviation of
+    all the block's samples over all frames. Computed in float64. Voxels no
+    block centres on are left at 0 (the reference leaves ``np.empty`` content
+    there, which is undefined).
+    """
+    x = np.asarray(noise_sequence)
+    x = x.astype(np.complex128 if np.iscomplexobj(x) else np.float64)
+    v_shape = x.shape[:-1]
+    b = int(block_size)
+    out = np.zeros(v_shape)
+    p_shape = (b,) * len(v_shape)
+    for tl in patch_locs(p_shape, (b - 1,) * len(v_shape), v_shape):
+        sl = tuple(slice(t, t + b) for t in tl)
+        ctr = tuple(int(t) + b // 2 for t in tl)
+        out[ctr] = np.std(x[sl])
+    return out
+
+
+def estimate_noise_covered(v_shape, block_size):
+    """Boolean map of the voxels ``estimate_noise`` writes (the block centres)."""
+    b = int(block_size)
+    cov = np.zeros(v_shape, dtype=bool)
+    sl = tuple(slice(b // 2, v - b + b // 2 + 1) for v in v_shape)
+    cov[sl] = True
+    return cov

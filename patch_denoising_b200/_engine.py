@@ -137,7 +137,42 @@ def to_host(tensors):
         hosts.append(h)
     if tensors:
         torch.cuda.current_stream(tensors[0].device).synchronize()
+    check_device_errors(block=True)
     return [h.numpy() for h in hosts]
+
+
+# Device-side error words (bounded waits that timed out) are read without
+# stalling the host: each call queues a copy of its words into pinned memory and
+# the check happens when that copy has landed -- at the next call, at the host
+# copy of the results, or at an explicit check_device_errors(block=True).
+_pending_errors = []
+
+
+def _queue_error_check(words, device):
+    h = torch.empty(len(words), dtype=torch.int32, pin_memory=True)
+    for i, w in enumerate(words):
+        h[i : i + 1].copy_(w[:4].view(torch.int32), non_blocking=True)
+    ev = torch.cuda.Event()
+    ev.record(torch.cuda.current_stream(device))
+    _pending_errors.append((ev, h))
+
+
+def check_device_errors(block: bool = False) -> None:
+    """Raise RuntimeError if a device-side wait of an earlier call timed out.
+
+    ``block``: wait for the pending checks instead of taking only the finished ones.
+    """
+    keep, code = [], 0
+    for ev, h in _pending_errors:
+        if block:
+            ev.synchronize()
+        elif not ev.query():
+            keep.append((ev, h))
+            continue
+        code = code or int(h.max())
+    _pending_errors[:] = keep
+    if code:
+        raise RuntimeError(f"a device-side wait timed out (code {code})")
 
 
 def run(
@@ -169,6 +204,7 @@ def run(
     device = data.device
     if device.type != "cuda":
         raise RuntimeError("the denoising path runs on a CUDA device only")
+    check_device_errors()
     cplx = data.is_complex()
     shape = tuple(data.shape)
     g = geometry(shape, p_s, p_o)
@@ -246,8 +282,7 @@ def run(
         lib.pd_finalize(gp, pp, _vp(out), _vp(wacc), _vp(nacc), _vp(nctr), _vp(weights), _vp(noise_map), _vp(mask),
                         mask_4d, s)
     )
-    if n_sel:
-        _lib.check(lib.pd_workspace_check(_vp(ws), s))
-    if mc_ws is not None:
-        _lib.check(lib.pd_workspace_check(_vp(mc_ws), s))
+    words = ([ws] if n_sel else []) + ([mc_ws] if mc_ws is not None else [])
+    if words:
+        _queue_error_check(words, device)
     return DeviceResult(out, weights, noise_map, rank_map, plist[:n_sel], prank[:n_sel], pnoise[:n_sel], level)

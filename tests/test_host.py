@@ -124,3 +124,30 @@ def test_patch_param_int_and_tuple():
     assert den._get_patch_param((64, 64, 20)) == ((6, 6, 20), (5, 5, 20))
     den = HybridPCADenoiser([3, 4, 5], (1, 1, 1))
     assert den._get_patch_param((10, 10, 10, 30)) == ((3, 4, 5, 30), (1, 1, 1, 30))
+
+
+def test_device_error_words_checked_without_a_stall():
+    """A queued error word raises once its copy has landed, and only then."""
+    import torch
+
+    from patch_denoising_b200 import _engine
+
+    class FakeEvent:
+        def __init__(self, done):
+            self.done = done
+
+        def query(self):
+            return self.done
+
+        def synchronize(self):
+            self.done = True
+
+    _engine._pending_errors[:] = [(FakeEvent(False), torch.tensor([0, 5], dtype=torch.int32))]
+    _engine.check_device_errors()  # copy not landed yet: nothing to report
+    assert len(_engine._pending_errors) == 1
+    with pytest.raises(RuntimeError, match="timed out"):
+        _engine.check_device_errors(block=True)
+    assert not _engine._pending_errors
+    _engine._pending_errors[:] = [(FakeEvent(True), torch.tensor([0, 0], dtype=torch.int32))]
+    _engine.check_device_errors()
+    assert not _engine._pending_errors
