@@ -186,6 +186,20 @@ pd_status pd_denoise_patches_noalloc(const pd_geometry* g, const pd_params* p, c
                                      void* d_out_acc, float* d_weight_acc, float* d_noise_acc, float* d_noise_ctr,
                                      int32_t* d_rank_map, int32_t* d_patch_rank, float* d_patch_noise, void* stream);
 
+/* Scratch bytes pd_estimate_noise needs (shape as for pd_estimate_noise). */
+pd_status pd_estimate_noise_workspace_size(int32_t ndim, const int64_t* shape, int32_t is_complex, size_t* bytes);
+
+/* Noise map of a noise-only sequence: for every block of block_size voxels per
+ * spatial axis (every position), the population standard deviation of the
+ * block's samples over all frames, written at the voxel block_size / 2 past the
+ * block's corner; other voxels get 0. shape = (spatial..., frames), 1 to 3
+ * spatial axes, each longer than block_size. d_in float32 or complex64 (is_complex),
+ * C order; d_noise_map float64 of the spatial shape.
+ * Replaces estimate_noise (space_time/utils.py:207-242). */
+pd_status pd_estimate_noise(int32_t ndim, const int64_t* shape, int32_t is_complex, const void* d_in,
+                            int32_t block_size, double* d_noise_map, void* d_workspace, size_t workspace_bytes,
+                            void* stream);
+
 /* Synchronise the stream and report whether any bounded device-side wait of the
  * last pd_denoise_patches call on this workspace timed out (PD_ERR_CUDA). */
 pd_status pd_workspace_check(const void* d_workspace, void* stream);

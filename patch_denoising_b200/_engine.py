@@ -286,3 +286,20 @@ def run(
     if words:
         _queue_error_check(words, device)
     return DeviceResult(out, weights, noise_map, rank_map, plist[:n_sel], prank[:n_sel], pnoise[:n_sel], level)
+
+
+def estimate_noise(data: torch.Tensor, block_size: int) -> torch.Tensor:
+    """``pd_estimate_noise`` on a device tensor (float32 or complex64, time last)."""
+    lib = _lib.load()
+    device = data.device
+    shape = tuple(int(v) for v in data.shape)
+    arr = (ctypes.c_int64 * len(shape))(*shape)
+    cplx = 1 if data.is_complex() else 0
+    need = ctypes.c_size_t()
+    _lib.check(lib.pd_estimate_noise_workspace_size(len(shape), arr, cplx, ctypes.byref(need)))
+    ws = torch.empty(max(need.value, 1), dtype=torch.uint8, device=device)
+    out = torch.empty(shape[:-1], dtype=torch.float64, device=device)
+    with torch.cuda.device(device):
+        _lib.check(lib.pd_estimate_noise(len(shape), arr, cplx, _vp(data), int(block_size), _vp(out), _vp(ws),
+                                         need.value, _stream(device)))
+    return out

@@ -497,6 +497,54 @@ pd_status pd_nordic_denoise_patches(const pd_geometry* g, const pd_params* p, do
                               d_level + 1);
 }
 
+// Spatial extents padded to 3 axes (block 1 on padded axes) and frame count.
+static pd_status noise_geometry(int32_t ndim, const int64_t* shape, int32_t block, int64_t dims[3], int blk[3],
+                                int* frames) {
+  if (!shape || ndim < 2 || ndim > 4) return fail(PD_ERR_INVALID, "need 1 to 3 spatial axes and a time axis");
+  if (block < 1) return fail(PD_ERR_INVALID, "block_size must be at least 1");
+  const int nsp = ndim - 1;
+  for (int i = 0; i < 3; ++i) {
+    dims[i] = i < nsp ? shape[i] : 1;
+    blk[i] = i < nsp ? block : 1;
+    if (i < nsp && shape[i] <= block)
+      return fail(PD_ERR_INVALID, "axis %d has %lld voxels, not more than block_size %d", i, (long long)shape[i],
+                  block);
+  }
+  if (shape[ndim - 1] < 1 || shape[ndim - 1] > INT32_MAX) return fail(PD_ERR_INVALID, "bad frame count");
+  *frames = (int)shape[ndim - 1];
+  return PD_OK;
+}
+
+pd_status pd_estimate_noise_workspace_size(int32_t ndim, const int64_t* shape, int32_t is_complex, size_t* bytes) {
+  g_err.clear();
+  if (!bytes) return fail(PD_ERR_INVALID, "NULL output");
+  int64_t dims[3];
+  int blk[3], T;
+  PD_TRY(noise_geometry(ndim, shape, 1, dims, blk, &T));
+  const size_t nvox = (size_t)(dims[0] * dims[1] * dims[2]);
+  *bytes = align256(sizeof(double) * nvox * (is_complex ? 2 : 1)) + align256(sizeof(double) * nvox);
+  return PD_OK;
+}
+
+pd_status pd_estimate_noise(int32_t ndim, const int64_t* shape, int32_t is_complex, const void* d_in,
+                            int32_t block_size, double* d_noise_map, void* d_ws, size_t ws_bytes, void* stream) {
+  g_err.clear();
+  int64_t dims[3];
+  int blk[3], T;
+  PD_TRY(noise_geometry(ndim, shape, block_size, dims, blk, &T));
+  if (!d_in || !d_noise_map) return fail(PD_ERR_INVALID, "NULL buffer");
+  size_t need;
+  PD_TRY(pd_estimate_noise_workspace_size(ndim, shape, is_complex, &need));
+  if (!d_ws || ws_bytes < need) return fail(PD_ERR_WORKSPACE, "workspace too small (%zu < %zu)", ws_bytes, need);
+  const size_t nvox = (size_t)(dims[0] * dims[1] * dims[2]);
+  Carver c(d_ws);
+  double* mean = c.take<double>(nvox * (is_complex ? 2 : 1));
+  double* m2 = c.take<double>(nvox);
+  launch_estimate_noise((const float*)d_in, is_complex != 0, dims, blk, T, mean, m2, d_noise_map,
+                        (cudaStream_t)stream);
+  return cuda_check(cudaGetLastError(), "pd_estimate_noise launch");
+}
+
 pd_status pd_workspace_check(const void* d_workspace, void* stream) {
   g_err.clear();
   if (!d_workspace) return fail(PD_ERR_INVALID, "NULL workspace");

@@ -96,6 +96,9 @@ int64_t mc_chunks(int64_t rows);
 void launch_gauss_fill(int64_t rows, int cols, uint64_t seed, int draw, float* out, cudaStream_t s);
 void launch_chunk_reduce(const float* part, int64_t part_stride, int chunks, int64_t np, int draws, float* gram,
                          int64_t gram_stride, cudaStream_t s);
+// pd_noise.cu
+void launch_estimate_noise(const float* in, bool cplx, const int64_t dims[3], const int blk[3], int T, double* mean,
+                           double* m2, double* out, cudaStream_t s);
 void launch_mc_level(const double* lam, int n_iter, double noise_std, double* out, cudaStream_t s);
 void launch_mc_gram(int64_t rows, int cols, int n_iter, uint64_t seed, float* part, float* gram,
                     int64_t gram_stride, cudaStream_t s);

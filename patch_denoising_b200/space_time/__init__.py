@@ -9,7 +9,7 @@ from .lowrank import (
     OptimalSVDDenoiser,
     RawSVDDenoiser,
 )
-from .utils import marchenko_pastur_median
+from .utils import estimate_noise, marchenko_pastur_median
 
 __all__ = [
     "BaseSpaceTimeDenoiser",
@@ -21,4 +21,5 @@ __all__ = [
     "OptimalSVDDenoiser",
     "AdaptiveDenoiser",
     "marchenko_pastur_median",
+    "estimate_noise",
 ]

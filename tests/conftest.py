@@ -23,6 +23,16 @@ def golden_names():
     return sorted(p.stem for p in GOLDEN.glob("*.npz"))
 
 
+def noise_golden_names():
+    return sorted(p.stem for p in (GOLDEN / "noise").glob("*.npz"))
+
+
+def load_noise_golden(name):
+    """(input, block_size, reference noise map, map of the voxels the reference writes)."""
+    z = np.load(GOLDEN / "noise" / f"{name}.npz", allow_pickle=False)
+    return z["input"], int(z["block_size"]), z["noise_map"], z["covered"]
+
+
 def load_golden(name):
     """Return (arrays, call) for a fixture; ``call`` holds oracle/denoiser kwargs."""
     z = np.load(GOLDEN / f"{name}.npz", allow_pickle=False)

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import golden_names, load_golden
+from conftest import golden_names, load_golden, load_noise_golden, noise_golden_names
 
 
 def _oracle_for(arrays, call):
@@ -42,3 +42,17 @@ def test_oracle_matches_reference(name):
     ok = ~np.isnan(gold)
     scale = np.max(np.abs(gold[ok])) if ok.any() else 1.0
     np.testing.assert_allclose(out[ok], gold[ok], rtol=1e-6, atol=1e-6 * scale)
+
+
+@pytest.mark.parametrize("name", noise_golden_names())
+def test_oracle_noise_map_matches_reference(name):
+    x, b, ref, covered = load_noise_golden(name)
+    ours = oracle.estimate_noise(x, b)
+    np.testing.assert_array_equal(oracle.estimate_noise_covered(x.shape[:-1], b), covered)
+    np.testing.assert_allclose(ours[covered], ref[covered], rtol=1e-13, atol=0)
+    assert np.all(ours[~covered] == 0)
+
+
+def test_oracle_noise_map_rejects_short_axes():
+    with pytest.raises(IndexError):
+        oracle.estimate_noise(np.zeros((3, 8, 8, 5)), 3)
