@@ -75,6 +75,32 @@ def test_config5_mppca_crop():
     compare(call, x)
 
 
+# ------------------------------------------------------- long series and max frames
+# Frames above the shared-memory limit of the eigensolver (complex T > 224, real
+# T > 300) keep the packed Gram in global memory and use the widest register
+# slot counts; with M < T the Grams are rank-deficient (T - M + 1 zero modes).
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_raw_complex_300_frames(precision):
+    x, _ = lowrank_volume((11, 10, 6, 300), 3, seed=21, complex_valued=True)
+    call = dict(method="raw", patch_shape=5, patch_overlap=2, recombination="weighted", threshold_value=250.0)
+    compare(call, x, precision=precision)
+
+
+@pytest.mark.parametrize("T", [224, 225, 448])
+def test_mppca_frames_up_to_max(T):
+    x, _ = lowrank_volume((8, 8, 6, T), 3, seed=T)
+    call = dict(method="mp-pca", patch_shape=5, patch_overlap=2, recombination="weighted", threshold_scale=1.0)
+    compare(call, x)
+
+
+@pytest.mark.parametrize("T", [224, 225, 320, 321])
+def test_optimal_complex_frame_boundaries(T):
+    # optimal shrinkage needs T <= M (the MP median's aspect ratio), so M = 7^3
+    x, _ = lowrank_volume((15, 15, 11, T), 2, seed=T + 1, complex_valued=True)
+    call = dict(method="optimal", patch_shape=7, patch_overlap=3, recombination="weighted", loss="nuc")
+    compare(call, x)
+
+
 def test_nordic_monte_carlo_level_statistics():
     rows, cols, n = 20000, 40, 10
     ours = _engine.nordic_max_sval(rows, cols, n, seed=7, device=torch.device("cuda", 0))
