@@ -5,7 +5,7 @@
 // writes, at the voxel b // 2 past the block's corner, the population standard
 // deviation of the block's samples over all frames. Here that is two passes:
 //   k_voxel_moments  a warp per voxel: mean and sum of squared deviations over
-//                    the frames, in FP64 (one read of the sequence, HBM-bound);
+//                    the frames from shifted FP64 sums (one read, HBM-bound);
 //   k_block_std      a thread per voxel: if it is a block centre, combine the
 //                    block's b^d voxel moments exactly (equal counts T:
 //                    M2 = sum_v [M2_v + T |mean_v - mean|^2]) and take
@@ -20,46 +20,44 @@
 
 namespace pd {
 
+// One read of each voxel's frames: sums of (x - x0) and |x - x0|^2 with x0 the
+// voxel's first frame (the shift keeps the FP64 moments exact to rounding for
+// any mean), then mean = x0 + S / T and M2 = Q - |S|^2 / T.
 template <bool CPLX>
 __global__ void __launch_bounds__(256) k_voxel_moments(const float* __restrict__ in, int64_t nvox, int T,
                                                        double* __restrict__ mean, double* __restrict__ m2) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t v = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; v < nvox; v += warps) {
-    double sr = 0.0, si = 0.0;
+    double sr = 0.0, si = 0.0, q = 0.0, x0r, x0i = 0.0;
     if constexpr (CPLX) {
       const float2* row = reinterpret_cast<const float2*>(in) + v * T;
+      const float2 f = row[0];
+      x0r = f.x;
+      x0i = f.y;
       for (int t = lane; t < T; t += 32) {
         const float2 x = row[t];
-        sr += x.x;
-        si += x.y;
-      }
-    } else {
-      const float* row = in + v * T;
-      for (int t = lane; t < T; t += 32) sr += row[t];
-    }
-    const double mr = warp_sum(sr) / T;
-    const double mi = CPLX ? warp_sum(si) / T : 0.0;
-    double q = 0.0;
-    if constexpr (CPLX) {
-      const float2* row = reinterpret_cast<const float2*>(in) + v * T;
-      for (int t = lane; t < T; t += 32) {
-        const float2 x = row[t];
-        const double dr = x.x - mr, di = x.y - mi;
+        const double dr = (double)x.x - x0r, di = (double)x.y - x0i;
+        sr += dr;
+        si += di;
         q += dr * dr + di * di;
       }
     } else {
       const float* row = in + v * T;
+      x0r = row[0];
       for (int t = lane; t < T; t += 32) {
-        const double dr = row[t] - mr;
+        const double dr = (double)row[t] - x0r;
+        sr += dr;
         q += dr * dr;
       }
     }
+    sr = warp_sum(sr);
+    if (CPLX) si = warp_sum(si);
     q = warp_sum(q);
     if (lane == 0) {
-      mean[(CPLX ? 2 : 1) * v] = mr;
-      if (CPLX) mean[2 * v + 1] = mi;
-      m2[v] = q;
+      mean[(CPLX ? 2 : 1) * v] = x0r + sr / T;
+      if (CPLX) mean[2 * v + 1] = x0i + si / T;
+      m2[v] = fmax(q - (sr * sr + si * si) / T, 0.0);
     }
   }
 }
