@@ -192,9 +192,10 @@ def algorithmic(kernel, n_patches, M, n, ranks):
 # DRAM bytes per launch from the ncu captures summarised under profiles/
 # (dram__bytes_read.sum + dram__bytes_write.sum of one launch).
 NCU_TRAFFIC = {
-    "eig": 65.276e6 + 0.242e6,  # profiles/k_eig_c64_n200_405patches.md
+    "eig": 65.277e6 + 0.140e6,  # profiles/k_eig_c64_n200_405patches.md
     "mc_gram_tc": 1.478e9 + 0.114e9,  # profiles/k_gram_tma_mc_draws_10x266200x200.md
-    "gauss_pack": 0.093e6 + 1.006e9,  # profiles/k_gauss_pack_10x266200x200.md
+    "gauss_pack": 0.025e6 + 1.007e9,  # profiles/k_gauss_pack_10x266200x200.md
+    "eig_mc": 0.846e6,  # profiles/k_top1_mc_draws_10x200.md
 }
 
 
