@@ -226,6 +226,17 @@ def roofline(name, per_launch_ms, launches, steps, work, kind, peaks):
             "per_launch_ms": per_launch_ms, "launches": launches}
 
 
+def max_over_ranks(value, dist, device):
+    """The largest per-rank value (the job's time), or ``value`` itself on one rank."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def ours_arm(args, rank, world):
     import torch
 
@@ -273,10 +284,7 @@ def ours_arm(args, rank, world):
             _lib.profile_enable(False)
         ms = ev0.elapsed_time(ev1) / args.steps
         ranks = den.patch_rank_.cpu().numpy()
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dist, dev)
         kern = _lib.profile_collect() if prof else {}
         return ms, kern, ranks
 
@@ -317,18 +325,20 @@ def ours_arm(args, rank, world):
         estimate_noise(xd, 3)
     _lib.profile_enable(False)
     nk = _lib.profile_collect()
-    nm_ms = sum(v[1] for k, v in nk.items() if k.startswith("noise")) / 10  # kernel time per call
+    nm_ms = max_over_ranks(sum(v[1] for k, v in nk.items() if k.startswith("noise")) / 10, dist, dev)
     nm_bytes = xd.numel() * xd.element_size() + 8 * xd[..., 0].numel()
 
     # end to end: NumPy in, NumPy out through the public API
     for i in range(2):  # hold results as the timed loop does, so both pinned output sets exist
         (out, w, nm, rm), _ = step(precision, x, i)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for i in range(args.steps):
         (out, w, nm, rm), _ = step(precision, x, 2000 + i)
     torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, dist, dev)
     h2d = x.nbytes
     d2h = out.nbytes + w.nbytes + nm.nbytes + rm.nbytes
 
