@@ -43,11 +43,6 @@ void launch_patch_mean(const Geo& g, bool cplx, const void* in, const PatchWork&
 void launch_prior(const Geo& g, int method, const double* noise_std, const PatchWork& w, cudaStream_t s);
 void launch_gram_fp32(const Geo& g, bool cplx, const void* in, const PatchWork& w, cudaStream_t s);
 
-// pd_gram_tc.cu (tcgen05)
-cudaError_t launch_gram_tc(const Geo& g, bool cplx, const void* in, const PatchWork& w, int split, int* err,
-                           cudaStream_t s);
-cudaError_t launch_dense_gram_tc(const float* mat, int64_t rows, int cols, int64_t rows_per_cta, float* part,
-                                 int64_t part_stride, int split, int* err, cudaStream_t s);
 // pd_eig.cu
 struct EigParams {
   int method;  // PD_METHOD_* or EIG_MODE_TOP1 (MC threshold)
@@ -93,7 +88,6 @@ cudaError_t launch_gauss_gram_packed(int64_t rows, int cols, int n_iter, uint64_
 
 // pd_mc.cu
 int64_t mc_chunks(int64_t rows);
-void launch_gauss_fill(int64_t rows, int cols, uint64_t seed, int draw, float* out, cudaStream_t s);
 void launch_chunk_reduce(const float* part, int64_t part_stride, int chunks, int64_t np, int draws, float* gram,
                          int64_t gram_stride, cudaStream_t s);
 // pd_noise.cu

@@ -100,29 +100,6 @@ __global__ void k_mc_reduce(const float* __restrict__ part, int64_t part_stride,
 
 int64_t mc_chunks(int64_t rows) { return (rows + MC_ROWS_PER_CTA - 1) / MC_ROWS_PER_CTA; }
 
-// Dense rows x cols standard Gaussian matrix of draw `draw` (same stream as k_mc_gram).
-__global__ void k_gauss_fill(int64_t rows, int cols, uint64_t seed, uint32_t draw, float* __restrict__ out) {
-  const int groups = (cols + 3) / 4;
-  const int64_t total = rows * groups;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = e / groups;
-    const int cg = (int)(e % groups);
-    float z[4];
-    normals4(seed, draw, (uint64_t)r, (uint32_t)cg, z);
-    float* o = out + r * cols + cg * 4;
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      if (cg * 4 + q < cols) o[q] = z[q];
-  }
-}
-
-void launch_gauss_fill(int64_t rows, int cols, uint64_t seed, int draw, float* out, cudaStream_t s) {
-  const int64_t total = rows * ((cols + 3) / 4);
-  int64_t blocks = (total + 255) / 256;
-  if (blocks > 148 * 64) blocks = 148 * 64;
-  PD_TIMED("gauss_fill", s, k_gauss_fill<<<(unsigned)blocks, 256, 0, s>>>(rows, cols, seed, (uint32_t)draw, out));
-}
-
 void launch_chunk_reduce(const float* part, int64_t part_stride, int chunks, int64_t np, int draws, float* gram,
                          int64_t gram_stride, cudaStream_t s) {
   dim3 rgrid((unsigned)((np + 255) / 256), draws);

@@ -99,15 +99,4 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
-// Byte offset of K-group g8 (8 bf16 = 16 B) of row `row` in a K-major SW128 tile
-// whose rows are 128 B (64 bf16) long.
-__device__ __forceinline__ uint32_t sw128_off(int row, int g8) {
-  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((g8 ^ (row & 7)) << 4));
-}
-
-__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
-  __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-  return *reinterpret_cast<uint32_t*>(&h);
-}
-
 }  // namespace pd
