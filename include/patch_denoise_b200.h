@@ -200,8 +200,10 @@ pd_status pd_estimate_noise(int32_t ndim, const int64_t* shape, int32_t is_compl
                             int32_t block_size, double* d_noise_map, void* d_workspace, size_t workspace_bytes,
                             void* stream);
 
-/* Synchronise the stream and report whether any bounded device-side wait of the
- * last pd_denoise_patches call on this workspace timed out (PD_ERR_CUDA). */
+/* Synchronise the stream and read the workspace's device error word from the
+ * last call on it: PD_ERR_INVALID if a processed patch holds a NaN or infinite
+ * sample (the reference's LAPACK calls raise ValueError on those), PD_ERR_CUDA
+ * if a bounded device-side wait timed out. */
 pd_status pd_workspace_check(const void* d_workspace, void* stream);
 
 /* Kernel timing (no reference counterpart; used by bench.py for the roofline).

@@ -157,8 +157,13 @@ def _queue_error_check(words, device):
     _pending_errors.append((ev, h))
 
 
+NONFINITE = 7  # error word of a processed patch with a NaN / inf sample (PD_DEVERR_NONFINITE)
+
+
 def check_device_errors(block: bool = False) -> None:
-    """Raise RuntimeError if a device-side wait of an earlier call timed out.
+    """Raise for an earlier call's device error word: ValueError for a NaN / inf
+    sample in a processed patch (the reference's LAPACK calls reject those),
+    RuntimeError for a timed-out device-side wait.
 
     ``block``: wait for the pending checks instead of taking only the finished ones.
     """
@@ -171,6 +176,8 @@ def check_device_errors(block: bool = False) -> None:
             continue
         code = code or int(h.max())
     _pending_errors[:] = keep
+    if code == NONFINITE:
+        raise ValueError("array must not contain infs or NaNs")
     if code:
         raise RuntimeError(f"a device-side wait timed out (code {code})")
 

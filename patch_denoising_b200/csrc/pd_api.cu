@@ -552,6 +552,7 @@ pd_status pd_workspace_check(const void* d_workspace, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   PD_TRY(cuda_check(cudaMemcpyAsync(&err, d_workspace, sizeof(int), cudaMemcpyDeviceToHost, s), "copy error word"));
   PD_TRY(cuda_check(cudaStreamSynchronize(s), "workspace check sync"));
+  if (err == PD_DEVERR_NONFINITE) return fail(PD_ERR_INVALID, "array must not contain infs or NaNs");
   if (err) return fail(PD_ERR_CUDA, "a device-side wait timed out (code %d)", err);
   return PD_OK;
 }

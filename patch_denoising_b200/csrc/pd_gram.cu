@@ -45,6 +45,10 @@ __global__ void __launch_bounds__(MEAN_THREADS) k_patch_mean(Geo g, const typena
     } else {
       mean[t] = (float)(sx / M);
     }
+    // A NaN or infinite sample makes the sum non-finite (float samples cannot
+    // overflow an FP64 sum): the reference's LAPACK calls reject such a patch
+    // ("array must not contain infs or NaNs"), so flag it.
+    if (!isfinite(sx) || !isfinite(sy)) atomicExch(w.err, PD_DEVERR_NONFINITE);
   }
 }
 

@@ -21,6 +21,10 @@ __global__ void k_scan_counts(int32_t* bc, int64_t nb, int32_t* total_out);
 __global__ void k_compact(const uint8_t* flags, int64_t n, const int32_t* boff, int32_t* list);
 
 // Per-patch work buffers for one chunk of listed patches.
+// Device error word codes (0 = ok): 4-6 a bounded TMA / MMA wait of the tensor-core
+// Gram timed out; PD_DEVERR_NONFINITE a processed patch holds a NaN or inf sample.
+constexpr int PD_DEVERR_NONFINITE = 7;
+
 struct PatchWork {
   const int32_t* list;  // linear patch indices of the chunk
   int32_t count;        // patches in the chunk

@@ -135,6 +135,27 @@ def test_nordic_level_on_device_matches_host_level(precision):
     assert rel_l2(w1.astype(np.float64), w2.astype(np.float64)) <= 1e-6
 
 
+def test_nonfinite_sample_in_a_processed_patch_raises():
+    """As the reference's SVD / eigh (check_finite): ValueError for NaN or inf in a
+    processed patch; none when the bad voxel lies only in masked-out patches."""
+    from patch_denoising_b200 import MPPCADenoiser, NordicDenoiser
+
+    x, _ = lowrank_volume((16, 16, 10, 30), 3, seed=31)
+    bad = x.copy()
+    bad[7, 7, 4, 3] = np.nan
+    with pytest.raises(ValueError, match="infs or NaNs"):
+        MPPCADenoiser(5, 2, threshold_scale=1.0).denoise(bad)
+    bad[7, 7, 4, 3] = np.inf
+    with pytest.raises(ValueError, match="infs or NaNs"):
+        NordicDenoiser(5, 2, precision="mixed").denoise(bad.astype(np.complex64), noise_std=1.0, mc_max_sval=1.0)
+    # outside every processed patch: the mask keeps only patches far from the bad voxel
+    mask = np.zeros(x.shape[:-1], dtype=bool)
+    mask[:5, :5, :5] = True
+    bad[15, 15, 9, 0] = np.nan
+    bad[7, 7, 4, 3] = 0.0
+    MPPCADenoiser(5, 2, threshold_scale=1.0).denoise(bad, mask=mask, mask_threshold=50)
+
+
 def test_torch_input_stays_on_device():
     x, _ = lowrank_volume((20, 20, 12, 40), 3, seed=8)
     xt = torch.from_numpy(x).cuda()

@@ -151,3 +151,22 @@ def test_device_error_words_checked_without_a_stall():
     _engine._pending_errors[:] = [(FakeEvent(True), torch.tensor([0, 0], dtype=torch.int32))]
     _engine.check_device_errors()
     assert not _engine._pending_errors
+
+
+def test_nonfinite_patch_word_raises_value_error():
+    """Error word 7 (a NaN / inf sample in a processed patch) is the reference's ValueError."""
+    import torch
+
+    from patch_denoising_b200 import _engine
+
+    class Done:
+        def query(self):
+            return True
+
+        def synchronize(self):
+            pass
+
+    _engine._pending_errors[:] = [(Done(), torch.tensor([7], dtype=torch.int32))]
+    with pytest.raises(ValueError, match="infs or NaNs"):
+        _engine.check_device_errors()
+    assert not _engine._pending_errors
