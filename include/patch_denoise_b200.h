@@ -160,6 +160,8 @@ pd_status pd_nordic_mc_threshold(int64_t rows, int64_t cols, int32_t n_iter, uin
  * p->method must be PD_METHOD_RAW; p->threshold is ignored.
  *   d_level   2 doubles on the device: [0] the level, [1] noise_std * level
  *   d_mc_ws   pd_nordic_workspace_size(mc_rows, g->cols, n_iter) bytes
+ *   mc_rows   0: no draws; d_level already holds the level of an earlier call
+ *             on the same stream (a volume processed in several patch ranges)
  * The other arguments are those of pd_denoise_patches (no noise map). Check
  * both workspaces with pd_workspace_check. Replaces NordicDenoiser.denoise's level
  * and patch loop (space_time/lowrank.py:221-246 and base.py:235-258). */

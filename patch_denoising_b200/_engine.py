@@ -310,3 +310,207 @@ def estimate_noise(data: torch.Tensor, block_size: int) -> torch.Tensor:
         _lib.check(lib.pd_estimate_noise(len(shape), arr, cplx, _vp(data), int(block_size), _vp(out), _vp(ws),
                                          need.value, _stream(device)))
     return out
+
+
+# --------------------------------------------------------------------------- #
+# Host (NumPy) volumes: upload, patch work and download overlap               #
+# --------------------------------------------------------------------------- #
+# A host volume at least this large, without a mask, is streamed: patches are
+# processed in ranges of patch-grid x positions (each range one eigensolver
+# wave), each range starts as soon as the x slabs it reads are on the device,
+# and the x slabs no later patch touches are normalised and copied back while
+# the next range runs. Uploads and downloads each have a stream of their own.
+STREAM_MIN_BYTES = 64 << 20
+_copy_streams = {}
+
+
+def _copy_stream(device, which):
+    """Per-device upload ("h2d") or download ("d2h") stream: separate, so the two
+    directions run on both copy engines at once."""
+    idx = device.index if device.index is not None else torch.cuda.current_device()
+    key = (idx, which)
+    if key not in _copy_streams:
+        _copy_streams[key] = torch.cuda.Stream(device)
+    return _copy_streams[key]
+
+
+def _params(method, recombination, loss, precision, cplx, has_prior, threshold_scale, threshold, mp_med):
+    prm = _lib.Params()
+    prm.method = _lib.METHOD[method]
+    prm.recombination = _lib.RECOMBINATION[recombination]
+    prm.loss = _lib.LOSS[loss]
+    prm.precision = _lib.PRECISION[precision]
+    prm.is_complex = 1 if cplx else 0
+    prm.has_prior = 1 if has_prior else 0
+    prm.threshold_scale = float(threshold_scale)
+    prm.threshold = float(threshold)
+    prm.mp_median = float(mp_med)
+    return prm
+
+
+def run_host(
+    method: str,
+    x: np.ndarray,
+    p_s,
+    p_o,
+    recombination: str,
+    mask_threshold: float,
+    *,
+    threshold_scale: float = 1.0,
+    threshold: float = 0.0,
+    noise_std: torch.Tensor | None = None,
+    loss: str = "fro",
+    mp_med: float = 0.0,
+    precision: str = "fp32",
+    nordic: dict | None = None,
+    device=None,
+):
+    """Denoise a host volume (float32 / complex64, C order, no mask) with streaming.
+
+    Returns ``(out, weights, noise_map, rank_map)`` as NumPy arrays (pinned
+    memory) and the DeviceResult of the per-patch records, or ``None`` when the
+    volume does not stream (then use ``to_device`` + ``run``).
+    """
+    lib = _lib.load()
+    if device is None:
+        device = torch.device("cuda", torch.cuda.current_device())
+    shape = tuple(x.shape)
+    cplx = np.iscomplexobj(x)
+    if x.nbytes < STREAM_MIN_BYTES or len(shape) != 4:
+        return None
+    g = geometry(shape, p_s, p_o)
+    gx = int(g.grid[0])
+    per_x = int(g.n_patches) // gx
+    n_sel = int(g.n_patches) if 100.0 > float(mask_threshold) else 0
+    if gx < 2 or n_sel == 0:
+        return None
+    check_device_errors()
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    xs_per = max(1, sms // per_x)  # x positions per range: at most one eigensolver wave
+    step_x, patch_x = int(g.step[0]), int(g.patch[0])
+    comp = torch.cuda.current_stream(device)
+    upl = _copy_stream(device, "h2d")
+    dnl = _copy_stream(device, "d2h")
+    s = ctypes.c_void_p(comp.cuda_stream)
+    gp = ctypes.byref(g)
+    tdtype = torch.complex64 if cplx else torch.float32
+
+    # identity patch list (no mask), accumulators, parameters: on the compute stream
+    need = ctypes.c_size_t()
+    _lib.check(lib.pd_select_workspace_size(gp, ctypes.byref(need)))
+    sel_ws = torch.empty(max(need.value, 1), dtype=torch.uint8, device=device)
+    plist = torch.empty(g.n_patches, dtype=torch.int32, device=device)
+    count = torch.zeros(1, dtype=torch.int32, device=device)
+    _lib.check(lib.pd_select_patches(gp, None, 0, float(mask_threshold), _vp(plist), _vp(count), _vp(sel_ws),
+                                     need.value, s))
+    prm = _params(method, recombination, loss, precision, cplx, noise_std is not None, threshold_scale, threshold,
+                  mp_med)
+    pp = ctypes.byref(prm)
+    nvox = shape[0] * shape[1] * shape[2]
+    ngt = int(g.grid[3])
+    out = torch.zeros(shape, dtype=tdtype, device=device)
+    wacc = torch.zeros(nvox * ngt, dtype=torch.float32, device=device)
+    nacc = torch.zeros_like(wacc)
+    nctr = torch.zeros(shape, dtype=torch.float32, device=device)
+    rank_map = torch.zeros(shape, dtype=torch.int32, device=device)
+    weights = torch.empty(shape, dtype=torch.float32, device=device)
+    noise_map = torch.empty(shape, dtype=torch.float32, device=device)
+    prank = torch.zeros(n_sel, dtype=torch.int32, device=device)
+    pnoise = torch.zeros(n_sel, dtype=torch.float32, device=device)
+    level = mc_ws = None
+    mc_need = ctypes.c_size_t()
+    if nordic is not None:
+        _lib.check(lib.pd_nordic_workspace_size(int(nordic["rows"]), int(g.cols), int(nordic["n_iter"]),
+                                                ctypes.byref(mc_need)))
+        mc_ws = torch.empty(max(mc_need.value, 1), dtype=torch.uint8, device=device)
+        level = torch.empty(2, dtype=torch.float64, device=device)
+
+    # host buffers of the results (pinned, returned as NumPy views)
+    h_out = torch.empty(shape, dtype=tdtype, pin_memory=True)
+    h_w = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+    h_nm = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+    h_rm = torch.empty(shape, dtype=torch.int32, pin_memory=True)
+
+    # upload state: the input goes up slab by slab on the copy stream
+    src = torch.from_numpy(x.reshape(-1).view(np.uint8))
+    dst = torch.empty(x.nbytes, dtype=torch.uint8, device=device)
+    data = dst.view(tdtype).view(shape)
+    slab = x.nbytes // shape[0]
+    stage_n = max(slab, (_STAGE_CHUNK // slab) * slab)
+    stage = [torch.empty(stage_n, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    done = [None, None]
+    up = {"bytes": 0, "k": 0}
+    upl.wait_stream(comp)  # buffers allocated on the compute stream
+    dnl.wait_stream(comp)
+
+    def upload_to(nbytes):
+        ev = None
+        while up["bytes"] < nbytes:
+            lo = up["bytes"]
+            hi = min(lo + stage_n, x.nbytes)
+            b = up["k"] & 1
+            if done[b] is not None:
+                done[b].synchronize()
+            stage[b][: hi - lo].copy_(src[lo:hi])
+            with torch.cuda.stream(upl):
+                dst[lo:hi].copy_(stage[b][: hi - lo], non_blocking=True)
+                done[b] = torch.cuda.Event()
+                done[b].record(upl)
+            up["bytes"], up["k"] = hi, up["k"] + 1
+            ev = done[b]
+        return ev
+
+    words = []
+    x_done = 0
+    for a in range(0, gx, xs_per):
+        b_ = min(gx, a + xs_per)
+        first, cnt = a * per_x, (b_ - a) * per_x
+        ev = upload_to(((b_ - 1) * step_x + patch_x) * slab)
+        if ev is not None:
+            comp.wait_event(ev)
+        _lib.check(lib.pd_denoise_workspace_size(gp, pp, cnt, ctypes.byref(need)))
+        ws = torch.empty(max(need.value, 1), dtype=torch.uint8, device=device)
+        words.append(ws)
+        lst = ctypes.c_void_p(plist.data_ptr() + 4 * first)
+        if nordic is None:
+            _lib.check(lib.pd_denoise_patches(
+                gp, pp, _vp(data), _vp(noise_std), lst, cnt, _vp(out), _vp(wacc), _vp(nacc), _vp(nctr),
+                _vp(rank_map), ctypes.c_void_p(prank.data_ptr() + 4 * first),
+                ctypes.c_void_p(pnoise.data_ptr() + 4 * first), _vp(ws), need.value, s))
+        else:
+            rows = int(nordic["rows"]) if a == 0 else 0  # later ranges reuse the level on the device
+            _lib.check(lib.pd_nordic_denoise_patches(
+                gp, pp, float(nordic["noise_std"]), rows, int(nordic["n_iter"]),
+                ctypes.c_uint64(int(nordic["seed"]) & (2**64 - 1)), _vp(level), _vp(mc_ws), mc_need.value,
+                _vp(data), lst, cnt, _vp(out), _vp(wacc), _vp(nacc), _vp(nctr), _vp(rank_map),
+                ctypes.c_void_p(prank.data_ptr() + 4 * first), ctypes.c_void_p(pnoise.data_ptr() + 4 * first),
+                _vp(ws), need.value, s))
+        # voxels below the next range's first patch are final: normalise and download them
+        x_end = b_ * step_x if b_ < gx else shape[0]
+        if x_end > x_done:
+            sub = _lib.Geometry.from_buffer_copy(g)
+            sub.shape[0] = x_end - x_done
+            v0 = x_done * shape[1] * shape[2]
+            e0 = v0 * shape[3]
+            _lib.check(lib.pd_finalize(
+                ctypes.byref(sub), pp, ctypes.c_void_p(out.data_ptr() + e0 * out.element_size()),
+                ctypes.c_void_p(wacc.data_ptr() + 4 * v0 * ngt), ctypes.c_void_p(nacc.data_ptr() + 4 * v0 * ngt),
+                ctypes.c_void_p(nctr.data_ptr() + 4 * e0), ctypes.c_void_p(weights.data_ptr() + 4 * e0),
+                ctypes.c_void_p(noise_map.data_ptr() + 4 * e0), None, 0, s))
+            fin = torch.cuda.Event()
+            fin.record(comp)
+            dnl.wait_event(fin)
+            with torch.cuda.stream(dnl):
+                for h, d in ((h_out, out), (h_w, weights), (h_nm, noise_map), (h_rm, rank_map)):
+                    h[x_done:x_end].copy_(d[x_done:x_end], non_blocking=True)
+            x_done = x_end
+    # the compute stream's later work (and buffer reuse) comes after both copy streams
+    comp.wait_stream(upl)
+    comp.wait_stream(dnl)
+    words = words + ([mc_ws] if mc_ws is not None else [])
+    _queue_error_check(words, device)
+    res = DeviceResult(out, weights, noise_map, rank_map, plist[:n_sel], prank, pnoise, level)
+    dnl.synchronize()
+    comp.synchronize()
+    check_device_errors(block=True)
+    return (h_out.numpy(), h_w.numpy(), h_nm.numpy(), h_rm.numpy()), res

@@ -486,11 +486,14 @@ pd_status pd_nordic_denoise_patches(const pd_geometry* g, const pd_params* p, do
   if (p->method != PD_METHOD_RAW) return fail(PD_ERR_INVALID, "pd_nordic_denoise_patches needs method RAW");
   if (!d_level) return fail(PD_ERR_INVALID, "NULL level output");
   cudaStream_t s = (cudaStream_t)stream;
-  // the draws, their Grams and top-1 eigenvalues, then the level and the threshold on the device
-  PatchWork mw;
-  PD_TRY(mc_launch(mc_rows, g->cols, n_iter, seed, p->precision, d_mc_ws, mc_ws_bytes, s, &mw));
-  launch_mc_level(mw.prior, n_iter, noise_std, d_level, s);
-  PD_TRY(cuda_check(cudaGetLastError(), "Monte-Carlo level launch"));
+  if (mc_rows < 0) return fail(PD_ERR_INVALID, "negative Monte-Carlo row count");
+  if (mc_rows > 0) {
+    // the draws, their Grams and top-1 eigenvalues, then the level and the threshold on the device
+    PatchWork mw;
+    PD_TRY(mc_launch(mc_rows, g->cols, n_iter, seed, p->precision, d_mc_ws, mc_ws_bytes, s, &mw));
+    launch_mc_level(mw.prior, n_iter, noise_std, d_level, s);
+    PD_TRY(cuda_check(cudaGetLastError(), "Monte-Carlo level launch"));
+  }
   // the patch loop reads the threshold from d_level[1]
   return denoise_patches_impl(g, p, d_in, nullptr, d_patch_list, n_selected, d_out_acc, d_weight_acc, d_noise_acc,
                               d_noise_ctr, d_rank_map, d_patch_rank, d_patch_noise, d_ws, ws_bytes, stream,

@@ -135,9 +135,26 @@ class BaseSpaceTimeDenoiser(abc.ABC):
         else:
             device = torch.device("cuda", torch.cuda.current_device())
         in_dtype = input_data.dtype
+        args = self._method_args(shape, p_s, device)
+        if not is_torch and mask is None:
+            # large host volumes stream: upload, patch ranges and download overlap
+            xh = np.ascontiguousarray(input_data)
+            if xh.dtype != np.dtype(_engine._NP[_engine.compute_dtype(in_dtype)]):
+                xh = xh.astype(_engine._NP[_engine.compute_dtype(in_dtype)])
+            with torch.cuda.device(device):
+                streamed = _engine.run_host(self._method, xh, p_s, p_o, self.recombination, mask_threshold,
+                                            precision=self.precision, device=device, **args)
+            if streamed is not None:
+                (out, weights, noise_map, rank_map), res = streamed
+                self.patch_index_ = res.patch_index.cpu().numpy()
+                self.patch_rank_ = res.patch_rank.cpu().numpy()
+                self.patch_noise_ = res.patch_noise.cpu().numpy()
+                self._take_result(res)
+                if np.dtype(in_dtype) != out.dtype:
+                    out = out.astype(in_dtype)
+                return out, weights, noise_map, rank_map
         x = _engine.to_device(input_data, device, _engine.compute_dtype(in_dtype))
         m = self._device_mask(mask, shape, device)
-        args = self._method_args(shape, p_s, device)
         with torch.cuda.device(device):
             res = _engine.run(self._method, x, p_s, p_o, self.recombination, m, mask_threshold,
                               precision=self.precision, **args)
