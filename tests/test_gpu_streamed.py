@@ -27,6 +27,9 @@ def _make(kind):
     if kind == "hybrid":
         x, _ = lowrank_volume((40, 24, 14, 60), 4, seed=42)
         return x, lambda: HybridPCADenoiser(5, 2, recombination="average"), {"noise_std": 5.0}
+    if kind == "mppca_time_tiled":
+        x, _ = lowrank_volume((40, 24, 14, 60), 4, seed=45)
+        return x, lambda: MPPCADenoiser((5, 5, 5, 20), (2, 2, 2, 10), threshold_scale=1.0), {}
     if kind == "optimal_center":
         x, _ = lowrank_volume((40, 24, 14, 60), 4, seed=43)
         return x, lambda: OptimalSVDDenoiser(7, 3, loss="nuc", recombination="center"), {}
@@ -34,7 +37,7 @@ def _make(kind):
     return x, lambda: NordicDenoiser(7, 3, precision="mixed"), {"noise_std": 5.0, "n_iter_threshold": 3}
 
 
-@pytest.mark.parametrize("kind", ["mppca", "hybrid", "optimal_center", "nordic_mixed"])
+@pytest.mark.parametrize("kind", ["mppca", "mppca_time_tiled", "hybrid", "optimal_center", "nordic_mixed"])
 def test_streamed_host_volume_matches_device_path(kind, monkeypatch):
     x, make, kw = _make(kind)
     monkeypatch.setattr(_engine, "STREAM_MIN_BYTES", 1 << 20)
