@@ -30,25 +30,38 @@ __global__ void __launch_bounds__(256) k_voxel_moments(const float* __restrict__
   const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t v = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; v < nvox; v += warps) {
     double sr = 0.0, si = 0.0, q = 0.0, x0r, x0i = 0.0;
+    // four loads in flight per lane before the FP64 arithmetic
     if constexpr (CPLX) {
       const float2* row = reinterpret_cast<const float2*>(in) + v * T;
       const float2 f = row[0];
       x0r = f.x;
       x0i = f.y;
-      for (int t = lane; t < T; t += 32) {
-        const float2 x = row[t];
-        const double dr = (double)x.x - x0r, di = (double)x.y - x0i;
-        sr += dr;
-        si += di;
-        q += dr * dr + di * di;
+      for (int t0 = lane; t0 < T; t0 += 128) {
+        float2 x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = (t0 + 32 * u < T) ? row[t0 + 32 * u] : f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const double dr = (double)x[u].x - x0r, di = (double)x[u].y - x0i;  // padding adds 0
+          sr += dr;
+          si += di;
+          q += dr * dr + di * di;
+        }
       }
     } else {
       const float* row = in + v * T;
-      x0r = row[0];
-      for (int t = lane; t < T; t += 32) {
-        const double dr = (double)row[t] - x0r;
-        sr += dr;
-        q += dr * dr;
+      const float f = row[0];
+      x0r = f;
+      for (int t0 = lane; t0 < T; t0 += 128) {
+        float x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = (t0 + 32 * u < T) ? row[t0 + 32 * u] : f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const double dr = (double)x[u] - x0r;  // padding adds 0
+          sr += dr;
+          q += dr * dr;
+        }
       }
     }
     sr = warp_sum(sr);
