@@ -101,6 +101,17 @@ def test_optimal_complex_frame_boundaries(T):
     compare(call, x)
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp32"])
+def test_config2_nordic_full_volume(precision):
+    """The benchmarked workload at full size (complex64 64x64x40x200, 405 patches of
+    1331 x 200) against the FP64 oracle at the same Monte-Carlo level."""
+    x, _ = lowrank_volume((64, 64, 40, 200), 6, noise=3.0, complex_valued=True, seed=2026)
+    call = dict(method="nordic", patch_shape=11, patch_overlap=5, recombination="weighted", noise_std=3.0)
+    mc = _engine.nordic_max_sval(11**3 * 200, 200, 10, seed=99, device=torch.device("cuda", 0),
+                                 precision=precision)
+    compare(call, x, precision=precision, nordic_max_sval=mc)
+
+
 def test_nordic_monte_carlo_level_statistics():
     rows, cols, n = 20000, 40, 10
     ours = _engine.nordic_max_sval(rows, cols, n, seed=7, device=torch.device("cuda", 0))
