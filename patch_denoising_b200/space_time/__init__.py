@@ -9,7 +9,15 @@ from .lowrank import (
     OptimalSVDDenoiser,
     RawSVDDenoiser,
 )
-from .utils import estimate_noise, marchenko_pastur_median
+from .utils import (
+    eig_analysis,
+    eig_synthesis,
+    estimate_noise,
+    get_patch_locs,
+    marchenko_pastur_median,
+    svd_analysis,
+    svd_synthesis,
+)
 
 __all__ = [
     "BaseSpaceTimeDenoiser",
@@ -22,4 +30,9 @@ __all__ = [
     "AdaptiveDenoiser",
     "marchenko_pastur_median",
     "estimate_noise",
+    "get_patch_locs",
+    "svd_analysis",
+    "svd_synthesis",
+    "eig_analysis",
+    "eig_synthesis",
 ]

@@ -42,8 +42,8 @@ def _accumulators(shape, grid_t, n_sel, dtype, dev):
 
 
 def _rel(a, b):
-    a = a.double().cpu().numpy().ravel()
-    b = b.double().cpu().numpy().ravel()
+    a = a.cpu().numpy().astype(np.complex128).ravel()
+    b = b.cpu().numpy().astype(np.complex128).ravel()
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
