@@ -51,15 +51,20 @@ __device__ __forceinline__ void pack_store(__nv_bfloat16* hi, __nv_bfloat16* lo,
   }
 }
 
-// grid: (patches, Kp / 64, ceil(N / 64)), 256 threads.
+// grid: patches x (Kp / 64) x ceil(N / 64) tiles flattened patch-major, so the
+// tiles of one patch (and of its neighbours, which share voxels) run close
+// together and the volume is read from DRAM about once; 256 threads.
 __global__ void __launch_bounds__(256) k_pack_patches(Geo g, const float* __restrict__ in, int N, int cplx,
                                                       const float* __restrict__ mean, const int32_t* __restrict__ list,
                                                       __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
                                                       int64_t kp) {
   __shared__ float tile[PK_R][PK_C + 1];
   __shared__ int64_t rb[PK_R];
-  const int p = blockIdx.x;
-  const int r0 = blockIdx.y * PK_R, c0 = blockIdx.z * PK_C;
+  const unsigned kt = (unsigned)(kp / PK_R), ct = (unsigned)((N + PK_C - 1) / PK_C);
+  const unsigned per = kt * ct;
+  const int p = (int)(blockIdx.x / per);
+  const unsigned t = blockIdx.x - (unsigned)p * per;
+  const int r0 = (int)(t % kt) * PK_R, c0 = (int)(t / kt) * PK_C;
   const int tid = threadIdx.x;
   int64_t o[4];
   patch_origin(g, list[p], o);
@@ -122,6 +127,7 @@ struct TmaArgs {
   int64_t kp;  // packed K extent
   int dense;   // 1: blockIdx.x is a K chunk of one operand per blockIdx.z
   int64_t k_per_cta;
+  int nblk;    // patch mode: Gram blocks per patch (grid = patches x nblk, flattened)
   float* out;
   int64_t out_stride;
   int* err;
@@ -165,15 +171,20 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
   uint64_t* done = bars + 2 * TM_STAGES;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
 
+  // patch mode: the blocks of one patch are consecutive in the flattened grid,
+  // so they share its operands in L2; dense mode: grid (chunks, blocks, draws)
+  const int nblk = a.dense ? 0 : a.nblk;
+  const int bidx = a.dense ? (int)blockIdx.y : (int)(blockIdx.x % (unsigned)nblk);
+  const int pidx = a.dense ? (int)blockIdx.x : (int)(blockIdx.x / (unsigned)nblk);
   int rb, nb, ncols;
-  tm_block_of(blockIdx.y, N, rb, nb, ncols);
+  tm_block_of(bidx, N, rb, nb, ncols);
   const int npad = (ncols + 15) & ~15;
   const int nbox = (npad + TM_BOX - 1) / TM_BOX;  // B boxes of 128 rows
   uint32_t tcols = 32;
   while (tcols < (uint32_t)npad) tcols <<= 1;
 
   int64_t k_begin = 0, k_end = a.kp;
-  int zc = blockIdx.x;  // third tensor-map coordinate: patch, or draw
+  int zc = pidx;  // third tensor-map coordinate: patch, or draw
   float* out;
   if (a.dense) {
     k_begin = (int64_t)blockIdx.x * a.k_per_cta;
@@ -181,7 +192,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
     zc = blockIdx.z;
     out = a.out + ((int64_t)blockIdx.z * gridDim.x + blockIdx.x) * a.out_stride;
   } else {
-    out = a.out + (int64_t)blockIdx.x * a.out_stride;
+    out = a.out + (int64_t)pidx * a.out_stride;
   }
   const int nch = (int)((k_end - k_begin + 63) / 64);
   const uint32_t tx_bytes = (split ? 2u : 1u) * (TM_TILE_A + (uint32_t)nbox * TM_BOX * 128u);
@@ -352,7 +363,10 @@ cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const Pa
   const int64_t kp = pack_k(g.rows);
   __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(packed);
   __nv_bfloat16* lo = hi + (int64_t)w.count * N * kp;
-  dim3 pg(w.count, (unsigned)(kp / PK_R), (N + PK_C - 1) / PK_C);
+  const int64_t tiles = (kp / PK_R) * ((N + PK_C - 1) / PK_C);
+  if ((int64_t)w.count * tiles > INT32_MAX || (int64_t)w.count * tm_blocks(N) > INT32_MAX)
+    return cudaErrorInvalidConfiguration;
+  const unsigned pg = (unsigned)(w.count * tiles);
   PD_TIMED("pack", s, k_pack_patches<<<pg, 256, 0, s>>>(g, (const float*)in, N, cplx ? 1 : 0, w.mean, w.list, hi, lo, kp));
   CUtensorMap mh, ml;
   cudaError_t e = make_map(&mh, hi, kp, N, w.count);
@@ -366,13 +380,14 @@ cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const Pa
   a.split = 3;
   a.kp = kp;
   a.dense = 0;
+  a.nblk = tm_blocks(N);
   a.out = w.gram;
   a.out_stride = w.gram_stride;
   a.err = w.err;
   const size_t smem = tm_smem(3);
   e = cudaFuncSetAttribute(k_gram_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid(w.count, tm_blocks(N));
+  const unsigned grid = (unsigned)(w.count * a.nblk);
   PD_TIMED("gram_tc", s, k_gram_tma<<<grid, TM_THREADS, smem, s>>>(mh, ml, a));
   return cudaGetLastError();
 }

@@ -197,58 +197,148 @@ void launch_synth(const Geo& g, bool cplx, const void* in, const PatchWork& w, c
 }
 
 // out /= weights (weighted / average), expand window sums to 4D, mask.
-template <bool CPLX>
-__global__ void k_finalize(Geo g, int recomb, typename Elem<CPLX>::T* __restrict__ out,
-                           const float* __restrict__ wacc, const float* __restrict__ nacc,
-                           const float* __restrict__ nctr, float* __restrict__ weights,
-                           float* __restrict__ noise_map, const uint8_t* __restrict__ mask, int mask_is_4d) {
+// A work item is FQ consecutive frames of one voxel: one index division per
+// item, and with T % FQ == 0 (VEC) every access is a 16-byte vector.
+constexpr int FQ = 4;
+
+template <bool CPLX, bool VEC, class I>
+__device__ __forceinline__ void finalize_items(const Geo& g, int recomb, typename Elem<CPLX>::T* __restrict__ out,
+                                               const float* __restrict__ wacc, const float* __restrict__ nacc,
+                                               const float* __restrict__ nctr, float* __restrict__ weights,
+                                               float* __restrict__ noise_map, const uint8_t* __restrict__ mask,
+                                               int mask_is_4d, I items, I groups) {
   using T = typename Elem<CPLX>::T;
-  const int64_t T4 = g.shape[3];
-  const int64_t total = g.shape[0] * g.shape[1] * g.shape[2] * T4;
-  const int64_t ngt = g.grid[3];
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t v = e / T4, t = e % T4;
-    float wsum = 0.f, nsum = 0.f;
-    for (int64_t k = 0; k < ngt; ++k) {
-      const int64_t t0 = k * g.step[3];
-      if (t >= t0 && t < t0 + g.patch[3]) {
-        wsum += wacc[v * ngt + k];
-        nsum += nacc[v * ngt + k];
+  const I T4 = (I)g.shape[3];
+  const int ngt = (int)g.grid[3];
+  for (I it = (I)blockIdx.x * blockDim.x + threadIdx.x; it < items; it += (I)gridDim.x * blockDim.x) {
+    const I v = it / groups;
+    const int t0 = (int)(it - v * groups) * FQ;
+    const int64_t e0 = (int64_t)v * T4 + t0;
+    float ws[FQ], ns[FQ];
+#pragma unroll
+    for (int q = 0; q < FQ; ++q) ws[q] = ns[q] = 0.f;
+    for (int k = 0; k < ngt; ++k) {
+      const int lo = k * (int)g.step[3], hi = lo + (int)g.patch[3];
+      if (t0 + FQ <= lo || t0 >= hi) continue;
+      const float wk = wacc[(int64_t)v * ngt + k], nk = nacc[(int64_t)v * ngt + k];
+#pragma unroll
+      for (int q = 0; q < FQ; ++q) {
+        if (t0 + q >= lo && t0 + q < hi) {
+          ws[q] += wk;
+          ns[q] += nk;
+        }
       }
     }
-    const bool m = mask == nullptr ? true : (mask_is_4d ? mask[e] != 0 : mask[v] != 0);
-    T val = out[e];
-    float nmap;
-    if (recomb != PD_RECOMB_CENTER) {
-      if constexpr (CPLX) val = cf{val.x / wsum, val.y / wsum};
-      else val = val / wsum;
-      nmap = nsum / wsum;
+    T val[FQ];
+    float nm[FQ];
+    bool keep[FQ];
+    if constexpr (VEC) {
+      if constexpr (CPLX) {
+        const float4 a = *reinterpret_cast<const float4*>(out + e0);
+        const float4 b = *reinterpret_cast<const float4*>(out + e0 + 2);
+        val[0] = cf{a.x, a.y};
+        val[1] = cf{a.z, a.w};
+        val[2] = cf{b.x, b.y};
+        val[3] = cf{b.z, b.w};
+      } else {
+        const float4 a = *reinterpret_cast<const float4*>(out + e0);
+        val[0] = a.x;
+        val[1] = a.y;
+        val[2] = a.z;
+        val[3] = a.w;
+      }
+      if (recomb == PD_RECOMB_CENTER) {
+        const float4 c = *reinterpret_cast<const float4*>(nctr + e0);
+        nm[0] = c.x;
+        nm[1] = c.y;
+        nm[2] = c.z;
+        nm[3] = c.w;
+      }
     } else {
-      nmap = nctr[e];
+#pragma unroll
+      for (int q = 0; q < FQ; ++q) {
+        val[q] = zero<T>();
+        nm[q] = 0.f;
+        if (t0 + q < T4) {
+          val[q] = out[e0 + q];
+          if (recomb == PD_RECOMB_CENTER) nm[q] = nctr[e0 + q];
+        }
+      }
     }
-    if (!m) {
-      val = zero<T>();
-      nmap = 0.f;
+#pragma unroll
+    for (int q = 0; q < FQ; ++q) {
+      keep[q] = mask == nullptr ? true : (mask_is_4d ? mask[e0 + q] != 0 : mask[v] != 0);
+      if (!VEC && t0 + q >= T4) keep[q] = false;
+      if (recomb != PD_RECOMB_CENTER) {
+        if constexpr (CPLX) val[q] = cf{val[q].x / ws[q], val[q].y / ws[q]};
+        else val[q] = val[q] / ws[q];
+        nm[q] = ns[q] / ws[q];
+      }
+      if (!keep[q]) {
+        val[q] = zero<T>();
+        nm[q] = 0.f;
+      }
     }
-    out[e] = val;
-    weights[e] = wsum;
-    noise_map[e] = nmap;
+    if constexpr (VEC) {
+      if constexpr (CPLX) {
+        *reinterpret_cast<float4*>(out + e0) = make_float4(val[0].x, val[0].y, val[1].x, val[1].y);
+        *reinterpret_cast<float4*>(out + e0 + 2) = make_float4(val[2].x, val[2].y, val[3].x, val[3].y);
+      } else {
+        *reinterpret_cast<float4*>(out + e0) = make_float4(val[0], val[1], val[2], val[3]);
+      }
+      *reinterpret_cast<float4*>(weights + e0) = make_float4(ws[0], ws[1], ws[2], ws[3]);
+      *reinterpret_cast<float4*>(noise_map + e0) = make_float4(nm[0], nm[1], nm[2], nm[3]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < FQ; ++q) {
+        if (t0 + q < T4) {
+          out[e0 + q] = val[q];
+          weights[e0 + q] = ws[q];
+          noise_map[e0 + q] = nm[q];
+        }
+      }
+    }
   }
+}
+
+template <bool CPLX, bool VEC>
+__global__ void __launch_bounds__(256) k_finalize(Geo g, int recomb, typename Elem<CPLX>::T* __restrict__ out,
+                                                  const float* __restrict__ wacc, const float* __restrict__ nacc,
+                                                  const float* __restrict__ nctr, float* __restrict__ weights,
+                                                  float* __restrict__ noise_map, const uint8_t* __restrict__ mask,
+                                                  int mask_is_4d) {
+  const int64_t groups = (g.shape[3] + FQ - 1) / FQ;
+  const int64_t items = g.shape[0] * g.shape[1] * g.shape[2] * groups;
+  if (items + (int64_t)gridDim.x * blockDim.x < (int64_t)0x7fffffff)
+    finalize_items<CPLX, VEC, int>(g, recomb, out, wacc, nacc, nctr, weights, noise_map, mask, mask_is_4d,
+                                   (int)items, (int)groups);
+  else
+    finalize_items<CPLX, VEC, int64_t>(g, recomb, out, wacc, nacc, nctr, weights, noise_map, mask, mask_is_4d,
+                                       items, groups);
 }
 
 void launch_finalize(const Geo& g, bool cplx, int recomb, void* out, const float* wacc, const float* nacc,
                      const float* nctr, float* weights, float* noise_map, const uint8_t* mask, int mask_is_4d,
                      cudaStream_t s) {
-  const int64_t total = g.shape[0] * g.shape[1] * g.shape[2] * g.shape[3];
-  int64_t blocks = (total + 255) / 256;
-  if (blocks > 148 * 32) blocks = 148 * 32;
-  if (cplx)
-    PD_TIMED("finalize", s, k_finalize<true><<<(int)blocks, 256, 0, s>>>(g, recomb, (cf*)out, wacc, nacc, nctr,
-                                                                         weights, noise_map, mask, mask_is_4d));
-  else
-    PD_TIMED("finalize", s, k_finalize<false><<<(int)blocks, 256, 0, s>>>(g, recomb, (float*)out, wacc, nacc, nctr,
-                                                                          weights, noise_map, mask, mask_is_4d));
+  const int64_t items = g.shape[0] * g.shape[1] * g.shape[2] * ((g.shape[3] + FQ - 1) / FQ);
+  int64_t blocks = (items + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  // 16-byte vectors need every item to start on a multiple of FQ frames and
+  // 16-byte aligned buffers
+  const auto al = [](const void* q) { return q == nullptr || (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+  const bool vec = g.shape[3] % FQ == 0 && al(out) && al(weights) && al(noise_map) && al(nctr);
+#define PD_FIN(C, V, TT)                                                                                      \
+  PD_TIMED("finalize", s, (k_finalize<C, V><<<(int)blocks, 256, 0, s>>>(g, recomb, (TT*)out, wacc, nacc, nctr, \
+                                                                         weights, noise_map, mask, mask_is_4d)))
+  if (cplx) {
+    if (vec) PD_FIN(true, true, cf);
+    else PD_FIN(true, false, cf);
+  } else {
+    if (vec) PD_FIN(false, true, float);
+    else PD_FIN(false, false, float);
+  }
+#undef PD_FIN
 }
 
 }  // namespace pd
