@@ -17,6 +17,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "pd_common.cuh"
@@ -51,46 +52,75 @@ __device__ __forceinline__ void pack_store(__nv_bfloat16* hi, __nv_bfloat16* lo,
   }
 }
 
-// grid: patches x (Kp / 64) x ceil(N / 64) tiles flattened patch-major, so the
-// tiles of one patch (and of its neighbours, which share voxels) run close
-// together and the volume is read from DRAM about once; 256 threads.
+// grid: patches x ceil(N / 64) column tiles x ks K segments, flattened
+// patch-major (a patch's CTAs, and its neighbours', which share voxels, run
+// close together, so the volume is read from DRAM about once); 256 threads.
+// A CTA walks the 64-voxel K tiles of its segment: the patch origin is
+// unravelled once, each tile's voxel offsets are formed one tile ahead, and the
+// next tile's loads are in flight while the current one is transposed
+// through shared memory and stored.
 __global__ void __launch_bounds__(256) k_pack_patches(Geo g, const float* __restrict__ in, int N, int cplx,
                                                       const float* __restrict__ mean, const int32_t* __restrict__ list,
                                                       __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
-                                                      int64_t kp) {
+                                                      int64_t kp, int ks) {
   __shared__ float tile[PK_R][PK_C + 1];
-  __shared__ int64_t rb[PK_R];
-  const unsigned kt = (unsigned)(kp / PK_R), ct = (unsigned)((N + PK_C - 1) / PK_C);
-  const unsigned per = kt * ct;
+  __shared__ int64_t rbs[2][PK_R];
+  const int kt_all = (int)(kp / PK_R), ct = (N + PK_C - 1) / PK_C;
+  const unsigned per = (unsigned)(ct * ks);
   const int p = (int)(blockIdx.x / per);
   const unsigned t = blockIdx.x - (unsigned)p * per;
-  const int r0 = (int)(t % kt) * PK_R, c0 = (int)(t / kt) * PK_C;
-  const int tid = threadIdx.x;
+  const int seg = (int)(t % (unsigned)ks), c0 = (int)(t / (unsigned)ks) * PK_C;
+  const int kt_per = (kt_all + ks - 1) / ks;
+  const int kt0 = seg * kt_per, kt1 = min(kt0 + kt_per, kt_all);
+  if (kt0 >= kt1) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int64_t o[4];
   patch_origin(g, list[p], o);
-  if (tid < PK_R) {
-    const int r = r0 + tid;
-    rb[tid] = r < g.rows ? (row_voxel(g, o, r) * g.shape[3] + o[3]) * (cplx ? 2 : 1) : -1;
-  }
-  __syncthreads();
+  const int64_t fs = cplx ? 2 : 1;
   const int c = tid % PK_C;
   const int col = c0 + c;
   const float mu = col < N ? mean[(int64_t)p * N + col] : 0.f;
-#pragma unroll 4
-  for (int rr = tid / PK_C; rr < PK_R; rr += 256 / PK_C) {
-    const int64_t base = rb[rr];
-    tile[rr][c] = (base >= 0 && col < N) ? __ldg(in + base + col) - mu : 0.f;
-  }
-  __syncthreads();
-  // each warp writes 64 K-values (128 B) of a column per step
-  const int warp = tid >> 5, lane = tid & 31;
   __nv_bfloat16* hp = hi + (int64_t)p * N * kp;
   __nv_bfloat16* lp = lo ? lo + (int64_t)p * N * kp : nullptr;
-  for (int cc = warp; cc < PK_C; cc += 8) {
-    const int colw = c0 + cc;
-    if (colw >= N) break;
-    const int64_t off = (int64_t)colw * kp + r0 + 2 * lane;
-    pack_store(hp, lp, off, tile[2 * lane][cc], tile[2 * lane + 1][cc]);
+  constexpr int RPT = PK_R / (256 / PK_C);  // rows loaded per thread and tile (16)
+  if (tid < PK_R) {
+    const int r = kt0 * PK_R + tid;
+    rbs[kt0 & 1][tid] = r < g.rows ? (row_voxel(g, o, r) * g.shape[3] + o[3]) * fs : -1;
+  }
+  __syncthreads();
+  float v[RPT];
+#pragma unroll
+  for (int i = 0; i < RPT; ++i) {
+    const int64_t base = rbs[kt0 & 1][tid / PK_C + i * (256 / PK_C)];
+    v[i] = (base >= 0 && col < N) ? __ldg(in + base + col) : 0.f;
+  }
+  for (int kt = kt0; kt < kt1; ++kt) {
+    if (tid < PK_R && kt + 1 < kt1) {
+      const int r = (kt + 1) * PK_R + tid;
+      rbs[(kt + 1) & 1][tid] = r < g.rows ? (row_voxel(g, o, r) * g.shape[3] + o[3]) * fs : -1;
+    }
+    __syncthreads();  // the previous tile has been read out of shared memory
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+      const int rr = tid / PK_C + i * (256 / PK_C);
+      tile[rr][c] = rbs[kt & 1][rr] >= 0 && col < N ? v[i] - mu : 0.f;
+    }
+    __syncthreads();  // tile kt and the offsets of tile kt + 1 are visible
+    if (kt + 1 < kt1) {
+#pragma unroll
+      for (int i = 0; i < RPT; ++i) {
+        const int64_t base = rbs[(kt + 1) & 1][tid / PK_C + i * (256 / PK_C)];
+        v[i] = (base >= 0 && col < N) ? __ldg(in + base + col) : 0.f;
+      }
+    }
+    // each warp writes 64 K-values (128 B) of a column per step
+    const int r0 = kt * PK_R;
+    for (int cc = warp; cc < PK_C; cc += 8) {
+      const int colw = c0 + cc;
+      if (colw >= N) break;
+      const int64_t off = (int64_t)colw * kp + r0 + 2 * lane;
+      pack_store(hp, lp, off, tile[2 * lane][cc], tile[2 * lane + 1][cc]);
+    }
   }
 }
 
@@ -363,11 +393,14 @@ cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const Pa
   const int64_t kp = pack_k(g.rows);
   __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(packed);
   __nv_bfloat16* lo = hi + (int64_t)w.count * N * kp;
-  const int64_t tiles = (kp / PK_R) * ((N + PK_C - 1) / PK_C);
-  if ((int64_t)w.count * tiles > INT32_MAX || (int64_t)w.count * tm_blocks(N) > INT32_MAX)
+  // K segments per column tile: enough CTAs for about eight waves of 8 per SM
+  const int64_t ktiles = kp / PK_R, ctiles = (N + PK_C - 1) / PK_C;
+  const int ks = (int)std::min<int64_t>(ktiles, std::max<int64_t>(1, (148 * 8 * 8) / ((int64_t)w.count * ctiles)));
+  if ((int64_t)w.count * ctiles * ks > INT32_MAX || (int64_t)w.count * tm_blocks(N) > INT32_MAX)
     return cudaErrorInvalidConfiguration;
-  const unsigned pg = (unsigned)(w.count * tiles);
-  PD_TIMED("pack", s, k_pack_patches<<<pg, 256, 0, s>>>(g, (const float*)in, N, cplx ? 1 : 0, w.mean, w.list, hi, lo, kp));
+  const unsigned pg = (unsigned)(w.count * ctiles * ks);
+  PD_TIMED("pack", s,
+           k_pack_patches<<<pg, 256, 0, s>>>(g, (const float*)in, N, cplx ? 1 : 0, w.mean, w.list, hi, lo, kp, ks));
   CUtensorMap mh, ml;
   cudaError_t e = make_map(&mh, hi, kp, N, w.count);
   if (e != cudaSuccess) return e;

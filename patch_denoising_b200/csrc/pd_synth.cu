@@ -25,7 +25,7 @@ __device__ __forceinline__ void acc_add(cf* p, cf v) {
 
 template <bool CPLX, int NS, int R>
 __global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
-                                                       PatchWork w, SynthArgs sa) {
+                                                       PatchWork w, SynthArgs sa, int ysplit) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ __align__(16) unsigned char sm[];
   const int n = g.cols, M = g.rows;
@@ -33,7 +33,11 @@ __global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Ele
   T* smean = ys + SYN_NW * R * n;    // [n]
   float* scoef = reinterpret_cast<float*>(smean + n);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int p = blockIdx.x;
+  // grid: patches x ysplit row blocks, flattened patch-major (the blocks of a
+  // patch, and of its overlapping neighbours, read and scatter to the same
+  // voxels close together in time)
+  const int p = (int)(blockIdx.x / (unsigned)ysplit);
+  const int yb = (int)(blockIdx.x - (unsigned)p * (unsigned)ysplit);
   const int64_t pidx = w.list[p];
   int64_t o[4];
   patch_origin(g, pidx, o);
@@ -51,7 +55,7 @@ __global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Ele
   const float theta = (sa.recombination == PD_RECOMB_WEIGHTED) ? (float)(1.0 / (2.0 + (double)rank)) : 1.f;
   const int rc = (int)(((g.patch[0] / 2) * g.patch[1] + g.patch[1] / 2) * g.patch[2] + g.patch[2] / 2);
   const int tc = (int)(g.patch[3] / 2);
-  if (blockIdx.y == 0 && tid == 0) {
+  if (yb == 0 && tid == 0) {
     sa.patch_rank[sa.list_offset + p] = rank;
     sa.patch_noise[sa.list_offset + p] = nv;
   }
@@ -62,9 +66,9 @@ __global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Ele
     else return vb[(int64_t)a * n2 + t];
   };
 
-  const int rstep = gridDim.y * SYN_NW * R;
-  int r0 = (blockIdx.y * SYN_NW + warp) * R;
-  if (center) r0 = (blockIdx.y == 0 && warp == 0) ? rc : M;  // one row only
+  const int rstep = ysplit * SYN_NW * R;
+  int r0 = (yb * SYN_NW + warp) * R;
+  if (center) r0 = (yb == 0 && warp == 0) ? rc : M;  // one row only
   for (; r0 < M; r0 += center ? M : rstep) {
     int64_t base[R];
     bool ok[R];
@@ -176,8 +180,8 @@ static void synth_ns(const Geo& g, const void* in, const PatchWork& w, const Syn
   int ysplit = (g.rows + rows_per_block - 1) / rows_per_block;
   if (ysplit > 8) ysplit = 8;
   if (a.recombination == PD_RECOMB_CENTER) ysplit = 1;
-  dim3 grid(w.count, ysplit);
-  PD_TIMED("synth_scatter", s, k_synth<CPLX, NS, R><<<grid, SYN_THREADS, smem, s>>>(g, (const T*)in, w, a));
+  const unsigned grid = (unsigned)((int64_t)w.count * ysplit);
+  PD_TIMED("synth_scatter", s, k_synth<CPLX, NS, R><<<grid, SYN_THREADS, smem, s>>>(g, (const T*)in, w, a, ysplit));
 }
 
 template <bool CPLX>
