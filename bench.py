@@ -177,7 +177,9 @@ def algorithmic(kernel, n_patches, M, n, ranks):
     if kernel == "eig":
         return 16.0 / 3.0 * n**3 * P, "flop"  # complex Householder tridiagonalisation
     if kernel == "synth_scatter":
-        return float(np.sum(16.0 * M * n * ranks)), "flop"
+        return 8.0 * M * n * P + 8.0 * M * n * P, "byte"  # complex rows in; theta-scaled rows scattered (atomics)
+    if kernel == "finalize":
+        return (8.0 + 8.0 + 4.0 + 4.0) * float(np.prod(SHAPE)), "byte"  # out read + written, weights, noise map
     if kernel == "gauss_pack":
         return 2.0 * N_ITER * M * n * n, "byte"  # bf16 normals written
     if kernel == "pack":
@@ -191,9 +193,14 @@ def algorithmic(kernel, n_patches, M, n, ranks):
 # (dram__bytes_read.sum + dram__bytes_write.sum of one launch).
 NCU_TRAFFIC = {
     "eig": 65.277e6 + 0.140e6,  # profiles/k_eig_c64_n200_405patches.md
-    "mc_gram_tc": 1.478e9 + 0.114e9,  # profiles/k_gram_tma_mc_draws_10x266200x200.md
+    "mc_gram_tc": 1.075e9 + 0.106e9,  # profiles/k_gram_tma_mc_draws_10x266200x200.md
     "gauss_pack": 0.025e6 + 1.007e9,  # profiles/k_gauss_pack_10x266200x200.md
     "eig_mc": 0.846e6,  # profiles/k_top1_mc_draws_10x200.md
+    # profiles/dram_traffic_pack_gram_synth_finalize_c64_64x64x40x200.md
+    "pack": 0.310e9 + 0.811e9,
+    "gram_tc": 0.871e9 + 0.059e9,
+    "synth_scatter": 0.392e9 + 0.150e9,
+    "finalize": 0.264e9 + 0.460e9,
 }
 
 

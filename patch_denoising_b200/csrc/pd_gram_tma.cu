@@ -155,9 +155,10 @@ struct TmaArgs {
   int cplx;
   int split;   // 3: hi/lo, 1: hi only
   int64_t kp;  // packed K extent
-  int dense;   // 1: blockIdx.x is a K chunk of one operand per blockIdx.z
+  int dense;   // 1: Grams of K chunks of dense draws (one partial per draw and chunk)
   int64_t k_per_cta;
-  int nblk;    // patch mode: Gram blocks per patch (grid = patches x nblk, flattened)
+  int nblk;    // Gram blocks per patch or per K chunk (grid flattened with the block fastest)
+  int chunks;  // dense: K chunks per draw
   float* out;
   int64_t out_stride;
   int* err;
@@ -201,11 +202,11 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
   uint64_t* done = bars + 2 * TM_STAGES;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
 
-  // patch mode: the blocks of one patch are consecutive in the flattened grid,
-  // so they share its operands in L2; dense mode: grid (chunks, blocks, draws)
-  const int nblk = a.dense ? 0 : a.nblk;
-  const int bidx = a.dense ? (int)blockIdx.y : (int)(blockIdx.x % (unsigned)nblk);
-  const int pidx = a.dense ? (int)blockIdx.x : (int)(blockIdx.x / (unsigned)nblk);
+  // The Gram blocks that read the same operand rows (of one patch, or of one
+  // K chunk of a draw) are consecutive in the flattened grid, so they share
+  // those rows in L2: patch mode (patch, block), dense mode (draw, chunk, block).
+  const int bidx = (int)(blockIdx.x % (unsigned)a.nblk);
+  const int pidx = (int)(blockIdx.x / (unsigned)a.nblk);
   int rb, nb, ncols;
   tm_block_of(bidx, N, rb, nb, ncols);
   const int npad = (ncols + 15) & ~15;
@@ -217,10 +218,11 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
   int zc = pidx;  // third tensor-map coordinate: patch, or draw
   float* out;
   if (a.dense) {
-    k_begin = (int64_t)blockIdx.x * a.k_per_cta;
+    const int chunk = pidx % a.chunks;  // pidx = draw * chunks + chunk
+    k_begin = (int64_t)chunk * a.k_per_cta;
     k_end = min(k_begin + a.k_per_cta, a.kp);
-    zc = blockIdx.z;
-    out = a.out + ((int64_t)blockIdx.z * gridDim.x + blockIdx.x) * a.out_stride;
+    zc = pidx / a.chunks;
+    out = a.out + (int64_t)pidx * a.out_stride;
   } else {
     out = a.out + (int64_t)pidx * a.out_stride;
   }
@@ -458,7 +460,10 @@ cudaError_t launch_gauss_gram_packed(int64_t rows, int cols, int n_iter, uint64_
   e = cudaFuncSetAttribute(k_gram_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int64_t chunks = (kp + a.k_per_cta - 1) / a.k_per_cta;
-  dim3 grid((unsigned)chunks, tm_blocks(cols), n_iter);
+  a.chunks = (int)chunks;
+  a.nblk = tm_blocks(cols);
+  if ((int64_t)n_iter * chunks * a.nblk > INT32_MAX) return cudaErrorInvalidConfiguration;
+  const unsigned grid = (unsigned)((int64_t)n_iter * chunks * a.nblk);
   PD_TIMED("mc_gram_tc", s, k_gram_tma<<<grid, TM_THREADS, smem, s>>>(mh, mh, a));
   return cudaGetLastError();
 }
