@@ -37,6 +37,14 @@ typedef int32_t pd_status;
 #define PD_METHOD_RAW 2     /* RawSVDDenoiser / NordicDenoiser hard threshold
                                (space_time/lowrank.py:123-246)                    */
 #define PD_METHOD_OPTIMAL 3 /* OptimalSVDDenoiser (space_time/lowrank.py:284-407) */
+#define PD_METHOD_ADAPTIVE 4 /* AdaptiveDenoiser  (space_time/lowrank.py:410-636):
+                                pd_adaptive_denoise_patches only                  */
+
+/* Adaptive trace-norm shrinkage d = s max(1 - (tau/s)^gamma, 0) (Josse & Sardy). */
+#define PD_ADAPTIVE_SURE 0  /* tau by SURE per candidate gamma, lowest cost wins */
+#define PD_ADAPTIVE_GSURE 1 /* the same with the generalised SURE cost           */
+#define PD_ADAPTIVE_QUT 2   /* tau = stdest * qut_level; gamma fixed or by SURE  */
+#define PD_ADAPTIVE_MAX_GAMMA 32
 
 #define PD_RECOMB_WEIGHTED 0 /* theta = 1 / (2 + maxidx)  (base.py:246-249) */
 #define PD_RECOMB_AVERAGE 1  /* theta = 1                 (base.py:250-252) */
@@ -73,6 +81,20 @@ typedef struct pd_params {
   double threshold;       /* raw / NORDIC singular-value threshold          */
   double mp_median;       /* optimal: Marchenko-Pastur median for beta      */
 } pd_params;
+
+/* Parameters of PD_METHOD_ADAPTIVE (AdaptiveDenoiser.denoise's tau0 / gamma0 and
+ * method, space_time/lowrank.py:546-605). */
+typedef struct pd_adaptive {
+  int32_t mode;     /* PD_ADAPTIVE_*                                                  */
+  int32_t n_gamma;  /* SURE / GSURE: candidates in gamma[] (1..PD_ADAPTIVE_MAX_GAMMA);
+                       QUT: 1 = gamma[0] is fixed, 0 = gamma estimated by SURE       */
+  int32_t has_tau0; /* SURE / GSURE: 1 = the log-tau search starts at tau0,
+                       0 = at log(median singular value)                             */
+  int32_t reserved;
+  double tau0;      /* log tau                                                        */
+  double qut_level; /* QUT: pd_adaptive_qut_level's quantile                          */
+  double gamma[PD_ADAPTIVE_MAX_GAMMA];
+} pd_adaptive;
 
 /* Library version (major*10000 + minor*100 + patch). */
 int32_t pd_version(void);
@@ -171,6 +193,34 @@ pd_status pd_nordic_denoise_patches(const pd_geometry* g, const pd_params* p, do
                                     int64_t n_selected, void* d_out_acc, float* d_weight_acc, float* d_noise_acc,
                                     float* d_noise_ctr, int32_t* d_rank_map, int32_t* d_patch_rank,
                                     float* d_patch_noise, void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* Quantile of the largest singular value of n_sim standard Gaussian rows x cols
+ * draws at probability 1 - 1/sqrt(log(max(rows, cols))) (numpy.quantile's
+ * linear interpolation), to *out. The reference draws n_sim matrices of the
+ * patch's shape scaled by its noise estimate for every patch and takes this
+ * quantile (space_time/lowrank.py:464-475); the quantile scales with the noise
+ * estimate, so one set of draws per call gives every patch's tau. The draws are
+ * pd_nordic_mc_threshold's (same seed convention and precision); workspace
+ * pd_nordic_workspace_size(rows, cols, n_sim). Synchronises the stream. */
+pd_status pd_adaptive_qut_level(int64_t rows, int64_t cols, int32_t n_sim, uint64_t seed, int32_t precision,
+                                double* out, void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* pd_denoise_patches for AdaptiveDenoiser (space_time/lowrank.py:607-636):
+ * p->method must be PD_METHOD_ADAPTIVE and p->has_prior 1, with d_noise_std
+ * the spatial noise_std map (the patch's noise estimate is
+ * sqrt(mean noise_std^2 over the patch)). Per patch the full singular
+ * spectrum comes from the Gram route; the SURE / GSURE cost
+ * (_sure_atn_cost, lowrank.py:410-447) is minimised over log tau (SURE /
+ * GSURE, every candidate gamma) or over log(gamma - 1) (QUT without a fixed
+ * gamma) by a bracketing line search and Brent's method on the device,
+ * in place of scipy.optimize.minimize (BFGS). Then d = s max(1 - (tau/s)^gamma, 0),
+ * maxidx = number of nonzero d. Workspace: pd_denoise_workspace_size. */
+pd_status pd_adaptive_denoise_patches(const pd_geometry* g, const pd_params* p, const pd_adaptive* a,
+                                      const void* d_in, const double* d_noise_std, const int32_t* d_patch_list,
+                                      int64_t n_selected, void* d_out_acc, float* d_weight_acc, float* d_noise_acc,
+                                      float* d_noise_ctr, int32_t* d_rank_map, int32_t* d_patch_rank,
+                                      float* d_patch_noise, void* d_workspace, size_t workspace_bytes,
+                                      void* stream);
 
 /* pd_denoise_patches without a workspace argument. No counterpart in the
  * reference. It is for callers that cannot allocate device memory while they

@@ -7,6 +7,7 @@ as the checker / the timed CPU reference arm.
 
 from .oracle import (  # noqa: F401
     METHODS,
+    atn_shrink,
     denoise,
     eig_analysis,
     eig_synthesis,
@@ -17,7 +18,9 @@ from .oracle import (  # noqa: F401
     nordic_threshold,
     patch_locs,
     patch_params,
+    qut_level,
     select_patches,
+    sure_atn_cost,
     svd_analysis,
     svd_synthesis,
 )

@@ -26,8 +26,9 @@ from __future__ import annotations
 import numpy as np
 from scipy.integrate import quad
 from scipy.linalg import eigh, svd
+from scipy.optimize import minimize
 
-METHODS = ("mp-pca", "hybrid-pca", "raw", "nordic", "optimal")
+METHODS = ("mp-pca", "hybrid-pca", "raw", "nordic", "optimal", "adaptive")
 
 # --------------------------------------------------------------------------- #
 # Patch geometry                                                              #
@@ -350,6 +351,217 @@ def _optimal_patch(x, loss, mp_median, sigma_prior=None, override=None):
 
 
 # --------------------------------------------------------------------------- #
+# Adaptive trace-norm shrinkage (AdaptiveDenoiser)                            #
+# --------------------------------------------------------------------------- #
+def sure_atn_cost(x_shape, method, s, gamma, sigma, tau):
+    """``_sure_atn_cost``, ``space_time/lowrank.py:410-447``: the (G)SURE cost of
+    the shrinkage d = s max(1 - (tau/s)^gamma, 0). For "qut" the variable is
+    log(gamma - 1), else log tau; the divergence matrix D is float32, as there."""
+    n_rows, n_cols = x_shape
+    if method == "qut":
+        gamma = np.exp(gamma) + 1
+    else:
+        tau = np.exp(tau)
+    s2 = s**2
+    d_hat = s * np.maximum(1 - (tau / s) ** gamma, 0)
+    sd = s * d_hat
+    dmat = np.zeros((len(s), len(s)), dtype=np.float32)
+    for i in range(len(s)):
+        gap = s2[i] - s2
+        gap[i] = np.inf
+        dmat[i, :] = sd[i] / gap
+    grad = (1 + (gamma - 1) * (tau / s) ** gamma) * (s >= tau)
+    div = np.sum(grad + abs(n_rows - n_cols) * d_hat / s) + 2 * np.sum(dmat)
+    rss = np.sum((d_hat - s) ** 2)
+    if method == "gsure":
+        return rss / (1 - div / n_rows / n_cols) ** 2
+    return sigma**2 * (-n_rows * n_cols + 2 * div) + rss
+
+
+def atn_shrink(s, gamma, tau):
+    """``_atn_shrink``, ``space_time/lowrank.py:459-461``."""
+    return s * np.maximum(1 - (tau / s) ** gamma, 0)
+
+
+def qut_level(x_shape, nbsim, rng=None):
+    """The QUT quantile for a unit noise estimate: ``_get_gamma_tau_qut``'s
+    ``maxd`` draws and quantile (``space_time/lowrank.py:466-475``) divided by stdest."""
+    rng = np.random if rng is None else rng
+    maxd = np.ones(nbsim)
+    for i in range(nbsim):
+        maxd[i] = np.max(svd(rng.randn(*x_shape), compute_uv=False, overwrite_a=True))
+    return np.quantile(maxd, 1 - 1 / np.sqrt(np.log(max(*x_shape))))
+
+
+def atn_cost64(s, si, x_shape, lt, gamma, sigma, gsure):
+    """The (G)SURE cost of ``sure_atn_cost`` at log tau = ``lt`` in float64, with
+    sum_ij D_ij = sum_i s_i d_i si_i (si_i = sum_{j != i} 1 / (s_i^2 - s_j^2)):
+    the form the library evaluates on the device."""
+    n_rows, n_cols = x_shape
+    tau = np.exp(lt)
+    r = np.exp(gamma * (lt - np.log(s)))
+    d_hat = s * np.maximum(1 - r, 0)
+    div = np.sum((1 + (gamma - 1) * r) * (s >= tau) + abs(n_rows - n_cols) * d_hat / s) + 2 * np.sum(s * d_hat * si)
+    rss = np.sum((d_hat - s) ** 2)
+    if gsure:
+        return rss / (1 - div / n_rows / n_cols) ** 2
+    return sigma**2 * (2 * div - n_rows * n_cols) + rss
+
+
+def _brent_min(f, a, b, tol=1e-10):
+    """Brent's minimisation on [a, b] (golden section with parabolic steps; Brent 1973, ch. 5)."""
+    cg = 0.3819660112501051
+    x = w = v = a + cg * (b - a)
+    fx = fw = fv = f(x)
+    d = e = 0.0
+    for _ in range(200):
+        m = 0.5 * (a + b)
+        tol1 = tol * abs(x) + 1e-12
+        tol2 = 2 * tol1
+        if abs(x - m) <= tol2 - 0.5 * (b - a):
+            break
+        golden = True
+        if abs(e) > tol1:
+            r = (x - w) * (fx - fv)
+            q = (x - v) * (fx - fw)
+            pp = (x - v) * q - (x - w) * r
+            q = 2 * (q - r)
+            if q > 0:
+                pp = -pp
+            else:
+                q = -q
+            e_old, e = e, d
+            if abs(pp) < abs(0.5 * q * e_old) and q * (a - x) < pp < q * (b - x):
+                d = pp / q
+                if (x + d) - a < tol2 or b - (x + d) < tol2:
+                    d = tol1 if x < m else -tol1
+                golden = False
+        if golden:
+            e = (b - x) if x < m else (a - x)
+            d = cg * e
+        u = x + d if abs(d) >= tol1 else x + (tol1 if d > 0 else -tol1)
+        fu = f(u)
+        if fu <= fx:
+            if u < x:
+                b = x
+            else:
+                a = x
+            v, fv, w, fw, x, fx = w, fw, x, fx, u, fu
+        else:
+            if u < x:
+                a = u
+            else:
+                b = u
+            if fu <= fw or w == x:
+                v, fv, w, fw = w, fw, u, fu
+            elif fu <= fv or v == x or v == w:
+                v, fv = u, fu
+    return x
+
+
+def line_search_min(f, x0, lo=-700.0, hi=700.0):
+    """The library's minimisation from x0 on [lo, hi]: forward-difference slope
+    (step 1.49e-8), first trial step -g min(1, 1.01/|g|) (as BFGS's first
+    line-search point), golden growth while the cost falls, then Brent inside
+    the bracket."""
+    h = 1.4901161193847656e-08
+    x0 = min(max(x0, lo), hi)
+    fa = f(x0)
+    g = (f(x0 + h) - fa) / h
+    if not abs(g) > 0:
+        return x0
+    a, b = x0, min(max(x0 - g * min(1.0, 1.01 / abs(g)), lo), hi)
+    if b == a:
+        return x0
+    fb = f(b)
+    if fb < fa:
+        c = min(max(b + 1.618033988749895 * (b - a), lo), hi)
+        fc = f(c)
+        for _ in range(60):
+            if not (fc < fb and c != b and lo < c < hi):
+                break
+            a, fa, b, fb = b, fb, c, fc
+            c = min(max(b + 1.618033988749895 * (b - a), lo), hi)
+            fc = f(c)
+        return _brent_min(f, min(a, c), max(a, c))
+    return _brent_min(f, min(a, b), max(a, b))
+
+
+def _adaptive_patch(x, stdest, method, gamma0, tau0, nbsim, qlevel=None, rng=None, override=None,
+                    optimizer="bfgs"):
+    """``AdaptiveDenoiser._patch_processing`` with ``_get_gamma_tau`` /
+    ``_get_gamma_tau_qut`` (``space_time/lowrank.py:464-533, 607-636``).
+    ``qlevel`` replaces the per-patch QUT draws (tau = stdest * qlevel).
+    ``optimizer="bfgs"``: scipy's BFGS on the float32-D cost, as the reference.
+    ``optimizer="search"``: the library's line search + Brent on the float64 cost
+    (``atn_cost64``), a deterministic function of the singular values."""
+    u, s, vt, mean = svd_analysis(x)
+    if optimizer == "search":
+        s = s.astype(np.float64)  # the cost in float64 whatever the patch's precision
+        s2 = s**2
+        with np.errstate(divide="ignore"):
+            si = np.array([np.sum(1.0 / (s2[k] - np.delete(s2, k))) for k in range(len(s))])
+        gs = method == "gsure"
+        if method == "qut":
+            tau = stdest * qlevel
+            if isinstance(gamma0, (float, np.floating)):
+                gamma = gamma0
+            else:
+                lt = np.log(tau)
+                gamma = np.exp(line_search_min(lambda g: atn_cost64(s, si, x.shape, lt, np.exp(g) + 1, stdest, gs),
+                                               0.0)) + 1
+        else:
+            x0 = np.log(np.median(s)) if tau0 is None else tau0
+            lo, hi = np.log(s[-1]) - 10.0, np.log(s[0]) + 10.0  # the library's bounds on log tau
+            best = np.inf
+            gamma, tau = gamma0[0], np.exp(x0)
+            for g in gamma0:
+                xt = line_search_min(lambda t: atn_cost64(s, si, x.shape, t, g, stdest, gs), x0, lo, hi)  # noqa: B023
+                cost = atn_cost64(s, si, x.shape, xt, g, stdest, gs)
+                if cost < best:
+                    gamma, tau, best = g, np.exp(xt), cost
+        return _adaptive_finish(x, u, s, vt, mean, gamma, tau, override)
+    if method == "qut":
+        if qlevel is None:
+            rng = np.random if rng is None else rng
+            maxd = np.ones(nbsim)
+            for i in range(nbsim):
+                maxd[i] = np.max(svd(rng.randn(*x.shape) * stdest, compute_uv=False, overwrite_a=True))
+            tau = np.quantile(maxd, 1 - 1 / np.sqrt(np.log(max(*x.shape))))
+        else:
+            tau = stdest * qlevel
+        if isinstance(gamma0, (float, np.floating)):
+            gamma = gamma0
+        else:
+            res = minimize(lambda g: sure_atn_cost(x.shape, "qut", s, g, stdest, tau), 0)
+            gamma = np.exp(res.x) + 1
+    else:
+        x0 = np.log(np.median(s)) if tau0 is None else tau0
+        best = np.inf
+        for g in gamma0:
+            res = minimize(lambda t: sure_atn_cost(x.shape, method, s, g, stdest, t), x0)  # noqa: B023
+            cost = sure_atn_cost(x.shape, method, s, g, stdest, res.x)
+            if cost < best:
+                gamma, tau, best = g, np.exp(res.x), cost
+    return _adaptive_finish(x, u, s, vt, mean, gamma, tau, override)
+
+
+def _adaptive_finish(x, u, s, vt, mean, gamma, tau, override):
+    """Shrink, maxidx, synthesis (``space_time/lowrank.py:626-636``); margin =
+    relative distance of the closest singular value to tau."""
+    shrunk = atn_shrink(s, gamma, tau)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        margin = float(np.min(np.abs(s / np.asarray(tau).reshape(-1)[0] - 1))) if len(s) else np.inf
+    rank = np.max(np.nonzero(shrunk)) + 1 if np.any(shrunk) else 0
+    if override is not None:
+        rank = np.int64(override) if override else 0
+        shrunk = shrunk.copy()
+        shrunk[rank:] = 0
+    new = np.zeros_like(x) + mean if rank == 0 else svd_synthesis(u, shrunk, vt, mean, rank)
+    return new, rank, np.nan, margin
+
+
+# --------------------------------------------------------------------------- #
 # Driver                                                                      #
 # --------------------------------------------------------------------------- #
 
@@ -381,13 +593,22 @@ def denoise(
     nordic_rng=None,
     threshold=None,
     rank_override=None,
+    adaptive_method="sure",
+    gamma0=None,
+    tau0=None,
+    nbsim=500,
+    qut_level=None,
+    adaptive_rng=None,
+    optimizer="bfgs",
 ):
     """Whole-volume denoising: ``BaseSpaceTimeDenoiser.denoise`` + method setup.
 
     Follows ``space_time/base.py:177-270`` for the driver and
     ``space_time/lowrank.py`` for the method set-up (``HybridPCADenoiser.denoise``
     :76-102, ``RawSVDDenoiser.denoise`` :142-168, ``NordicDenoiser.denoise``
-    :197-246, ``OptimalSVDDenoiser.denoise`` :318-377).
+    :197-246, ``OptimalSVDDenoiser.denoise`` :318-377, ``AdaptiveDenoiser.denoise``
+    :563-605 with ``adaptive_method``, ``gamma0``, ``tau0``, ``nbsim``; ``qut_level``
+    replaces the per-patch QUT draws; ``optimizer`` as for ``_adaptive_patch``).
 
     ``threshold`` (raw / nordic) replaces the computed singular-value threshold.
     Returns a dict with the reference outputs ``out``, ``weights`` and the
@@ -426,6 +647,8 @@ def denoise(
         mp_med = marchenko_pastur_median(p_s[-1] / np.prod(p_s[:-1]), eps=eps_marshenko_pastur)
         if noise_std is not None:
             prior = _prior_patches(noise_std, data_shape)
+    elif method == "adaptive":
+        prior = _prior_patches(noise_std, data_shape)
 
     # ---- driver (base.py:193-270) ------------------------------------------
     out = np.zeros(data_shape, dtype=data.dtype)
@@ -451,6 +674,9 @@ def denoise(
             new, rank, nvar, marg = _hybrid_patch(x, np.mean(prior[sl]), ov)
         elif method in ("raw", "nordic"):
             new, rank, nvar, marg = _raw_patch(x, thr, ov)
+        elif method == "adaptive":
+            new, rank, nvar, marg = _adaptive_patch(x, np.sqrt(np.mean(prior[sl])), adaptive_method, gamma0, tau0,
+                                                    nbsim, qut_level, adaptive_rng, ov, optimizer)
         else:
             sig = None if prior is None else np.mean(np.sqrt(prior[sl]))
             new, rank, nvar, marg = _optimal_patch(x, loss, mp_med, sig, ov)

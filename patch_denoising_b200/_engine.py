@@ -61,6 +61,36 @@ def nordic_max_sval(rows: int, cols: int, n_iter: int, seed: int, device, precis
     return out.value
 
 
+def adaptive_qut_level(rows: int, cols: int, n_sim: int, seed: int, device, precision: str = "fp32") -> float:
+    """QUT quantile of the largest singular value of ``n_sim`` Gaussian rows x cols draws."""
+    lib = _lib.load()
+    need = ctypes.c_size_t()
+    _lib.check(lib.pd_nordic_workspace_size(int(rows), int(cols), int(n_sim), ctypes.byref(need)))
+    ws = torch.empty(max(need.value, 1), dtype=torch.uint8, device=device)
+    out = ctypes.c_double()
+    _lib.check(
+        lib.pd_adaptive_qut_level(
+            int(rows), int(cols), int(n_sim), ctypes.c_uint64(int(seed) & (2**64 - 1)),
+            _lib.PRECISION[precision], ctypes.byref(out), _vp(ws), need.value, _stream(device),
+        )
+    )
+    return out.value
+
+
+def _adaptive_struct(adaptive: dict):
+    ad = _lib.Adaptive()
+    ad.mode = _lib.ADAPTIVE_MODE[adaptive["mode"]]
+    gam = list(adaptive.get("gamma") or [])
+    ad.n_gamma = len(gam)
+    for i, v in enumerate(gam):
+        ad.gamma[i] = float(v)
+    tau0 = adaptive.get("tau0")
+    ad.has_tau0 = 0 if tau0 is None else 1
+    ad.tau0 = 0.0 if tau0 is None else float(tau0)
+    ad.qut_level = float(adaptive.get("qut_level") or 0.0)
+    return ad
+
+
 @dataclass
 class DeviceResult:
     """Outputs of one call, on the device."""
@@ -198,6 +228,7 @@ def run(
     mp_med: float = 0.0,
     precision: str = "fp32",
     nordic: dict | None = None,
+    adaptive: dict | None = None,
 ) -> DeviceResult:
     """Denoise ``data`` (device tensor, float32 or complex64, C-contiguous).
 
@@ -206,6 +237,8 @@ def run(
     ``nordic``: {"noise_std", "rows", "n_iter", "seed"}: compute the NORDIC
     Monte-Carlo level on the device ahead of the patch loop, with no host
     round trip (``pd_nordic_denoise_patches``); ``threshold`` is then unused.
+    ``adaptive``: {"mode", "gamma", "tau0", "qut_level"} for the adaptive
+    shrinkage (``pd_adaptive_denoise_patches``).
     """
     lib = _lib.load()
     device = data.device
@@ -263,7 +296,15 @@ def run(
     _lib.check(lib.pd_denoise_workspace_size(gp, pp, n_sel, ctypes.byref(need)))
     ws = torch.empty(max(need.value, 1), dtype=torch.uint8, device=device)
     level = mc_ws = None
-    if nordic is None:
+    if adaptive is not None:
+        ad = _adaptive_struct(adaptive)
+        _lib.check(
+            lib.pd_adaptive_denoise_patches(
+                gp, pp, ctypes.byref(ad), _vp(data), _vp(noise_std), _vp(plist), n_sel, _vp(out), _vp(wacc),
+                _vp(nacc), _vp(nctr), _vp(rank_map), _vp(prank), _vp(pnoise), _vp(ws), need.value, s,
+            )
+        )
+    elif nordic is None:
         _lib.check(
             lib.pd_denoise_patches(
                 gp, pp, _vp(data), _vp(noise_std), _vp(plist), n_sel, _vp(out), _vp(wacc), _vp(nacc), _vp(nctr),
@@ -363,6 +404,7 @@ def run_host(
     mp_med: float = 0.0,
     precision: str = "fp32",
     nordic: dict | None = None,
+    adaptive: dict | None = None,
     device=None,
 ):
     """Denoise a host volume (float32 / complex64, C order, no mask) with streaming.
@@ -376,7 +418,7 @@ def run_host(
         device = torch.device("cuda", torch.cuda.current_device())
     shape = tuple(x.shape)
     cplx = np.iscomplexobj(x)
-    if x.nbytes < STREAM_MIN_BYTES or len(shape) != 4:
+    if x.nbytes < STREAM_MIN_BYTES or len(shape) != 4 or adaptive is not None:
         return None
     g = geometry(shape, p_s, p_o)
     gx = int(g.grid[0])

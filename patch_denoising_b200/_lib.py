@@ -19,7 +19,9 @@ PD_ERR_UNSUPPORTED = 2
 PD_ERR_CUDA = 3
 PD_ERR_WORKSPACE = 4
 
-METHOD = {"mp-pca": 0, "hybrid-pca": 1, "raw": 2, "nordic": 2, "optimal": 3}
+METHOD = {"mp-pca": 0, "hybrid-pca": 1, "raw": 2, "nordic": 2, "optimal": 3, "adaptive": 4}
+ADAPTIVE_MODE = {"sure": 0, "gsure": 1, "qut": 2}
+ADAPTIVE_MAX_GAMMA = 32
 RECOMBINATION = {"weighted": 0, "average": 1, "center": 2}
 LOSS = {"fro": 0, "nuc": 1, "ope": 2}
 PRECISION = {"fp32": 0, "mixed": 1}
@@ -57,8 +59,23 @@ class Params(ctypes.Structure):
     ]
 
 
+class Adaptive(ctypes.Structure):
+    """``pd_adaptive``."""
+
+    _fields_ = [
+        ("mode", c_i32),
+        ("n_gamma", c_i32),
+        ("has_tau0", c_i32),
+        ("reserved", c_i32),
+        ("tau0", c_dbl),
+        ("qut_level", c_dbl),
+        ("gamma", c_dbl * 32),
+    ]
+
+
 G_P = ctypes.POINTER(Geometry)
 P_P = ctypes.POINTER(Params)
+A_P = ctypes.POINTER(Adaptive)
 
 # name -> (restype, argtypes); every symbol declared in include/patch_denoise_b200.h
 SIGNATURES = {
@@ -80,6 +97,11 @@ SIGNATURES = {
         c_i32,
         [G_P, P_P, c_dbl, c_i64, c_i32, ctypes.c_uint64, c_vp, c_vp, c_sz, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp,
          c_vp, c_vp, c_vp, c_vp, c_vp, c_sz, c_vp],
+    ),
+    "pd_adaptive_qut_level": (c_i32, [c_i64, c_i64, c_i32, ctypes.c_uint64, c_i32, ctypes.POINTER(c_dbl), c_vp, c_sz, c_vp]),
+    "pd_adaptive_denoise_patches": (
+        c_i32,
+        [G_P, P_P, A_P, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_sz, c_vp],
     ),
     "pd_denoise_patches_noalloc": (
         c_i32,

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <string>
+#include <vector>
 
 #include "pd_common.cuh"
 #include "pd_kernels.cuh"
@@ -117,7 +118,7 @@ pd_status check_geometry(const pd_geometry* g) {
 
 pd_status check_params(const pd_geometry* g, const pd_params* p) {
   if (!p) return fail(PD_ERR_INVALID, "params is NULL");
-  if (p->method < PD_METHOD_MPPCA || p->method > PD_METHOD_OPTIMAL)
+  if (p->method < PD_METHOD_MPPCA || p->method > PD_METHOD_ADAPTIVE)
     return fail(PD_ERR_INVALID, "unknown method %d", p->method);
   if (p->recombination < PD_RECOMB_WEIGHTED || p->recombination > PD_RECOMB_CENTER)
     return fail(PD_ERR_INVALID, "recombination must be one of 'weighted', 'average', 'center'");
@@ -328,14 +329,19 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
                                       const double* d_noise_std, const int32_t* d_patch_list, int64_t n_selected,
                                       void* d_out_acc, float* d_weight_acc, float* d_noise_acc, float* d_noise_ctr,
                                       int32_t* d_rank_map, int32_t* d_patch_rank, float* d_patch_noise, void* d_ws,
-                                      size_t ws_bytes, void* stream, const double* d_thr) {
+                                      size_t ws_bytes, void* stream, const double* d_thr,
+                                      const pd_adaptive* ad = nullptr) {
   PD_TRY(check_geometry(g));
   PD_TRY(check_params(g, p));
+  if ((p->method == PD_METHOD_ADAPTIVE) != (ad != nullptr))
+    return fail(PD_ERR_INVALID, "PD_METHOD_ADAPTIVE runs through pd_adaptive_denoise_patches only");
   if (n_selected == 0) return PD_OK;
   if (!d_in || !d_patch_list || !d_out_acc || !d_weight_acc || !d_noise_acc || !d_noise_ctr || !d_rank_map ||
       !d_patch_rank || !d_patch_noise)
     return fail(PD_ERR_INVALID, "NULL buffer");
-  if ((p->method == PD_METHOD_HYBRID || (p->method == PD_METHOD_OPTIMAL && p->has_prior)) && !d_noise_std)
+  if ((p->method == PD_METHOD_HYBRID || p->method == PD_METHOD_ADAPTIVE ||
+       (p->method == PD_METHOD_OPTIMAL && p->has_prior)) &&
+      !d_noise_std)
     return fail(PD_ERR_INVALID, "this method needs the noise_std map");
   const int n = (int)g->cols;
   const bool cplx = p->is_complex != 0;
@@ -365,13 +371,14 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
     PatchWork w = carve_work(d_ws, cnt, n, cplx, &used, pk_b);
     w.list = d_patch_list + off;
     launch_patch_mean(G, cplx, d_in, w, s);
-    if (p->method == PD_METHOD_HYBRID || (p->method == PD_METHOD_OPTIMAL && p->has_prior))
+    if (p->method == PD_METHOD_HYBRID || p->method == PD_METHOD_ADAPTIVE ||
+        (p->method == PD_METHOD_OPTIMAL && p->has_prior))
       launch_prior(G, p->method, d_noise_std, w, s);
     if (p->precision == PD_PRECISION_MIXED)
       PD_TRY(cuda_check(launch_gram_packed(G, cplx, d_in, w, w.packed, s), "tensor-core Gram launch"));
     else
       launch_gram_fp32(G, cplx, d_in, w, s);
-    PD_TRY(cuda_check(launch_eig(cplx, n, ep, w, s), "eigensolver launch"));
+    PD_TRY(cuda_check(launch_eig(cplx, n, ep, w, s, ad), "eigensolver launch"));
     SynthArgs sa;
     sa.recombination = p->recombination;
     sa.out = d_out_acc;
@@ -498,6 +505,56 @@ pd_status pd_nordic_denoise_patches(const pd_geometry* g, const pd_params* p, do
   return denoise_patches_impl(g, p, d_in, nullptr, d_patch_list, n_selected, d_out_acc, d_weight_acc, d_noise_acc,
                               d_noise_ctr, d_rank_map, d_patch_rank, d_patch_noise, d_ws, ws_bytes, stream,
                               d_level + 1);
+}
+
+pd_status pd_adaptive_qut_level(int64_t rows, int64_t cols, int32_t n_sim, uint64_t seed, int32_t precision,
+                                double* out, void* d_ws, size_t ws_bytes, void* stream) {
+  g_err.clear();
+  if (!out) return fail(PD_ERR_INVALID, "NULL output");
+  if (n_sim < 1) return fail(PD_ERR_INVALID, "nbsim must be at least 1");
+  cudaStream_t s = (cudaStream_t)stream;
+  PatchWork w;
+  PD_TRY(mc_launch(rows, cols, n_sim, seed, precision, d_ws, ws_bytes, s, &w));
+  std::vector<double> lam((size_t)n_sim);
+  PD_TRY(cuda_check(cudaMemcpyAsync(lam.data(), w.prior, sizeof(double) * n_sim, cudaMemcpyDeviceToHost, s),
+                    "copy"));
+  PD_TRY(cuda_check(cudaStreamSynchronize(s), "Monte-Carlo sync"));
+  int err = 0;
+  PD_TRY(cuda_check(cudaMemcpy(&err, w.err, sizeof(int), cudaMemcpyDeviceToHost), "copy error word"));
+  if (err) return fail(PD_ERR_CUDA, "a device-side wait timed out (code %d)", err);
+  // numpy.quantile(maxd, q), default linear method: sorted v, h = (N - 1) q,
+  // v[floor h] + (h - floor h) (v[floor h + 1] - v[floor h])
+  for (auto& v : lam) v = sqrt(fmax(v, 0.0));
+  std::sort(lam.begin(), lam.end());
+  const double q = 1.0 - 1.0 / sqrt(log((double)std::max(rows, cols)));
+  const double h = (double)(n_sim - 1) * q;
+  const int64_t lo = std::min<int64_t>(std::max<int64_t>((int64_t)floor(h), 0), n_sim - 1);
+  const int64_t hi = std::min<int64_t>(lo + 1, n_sim - 1);
+  *out = lam[lo] + (h - (double)lo) * (lam[hi] - lam[lo]);
+  return PD_OK;
+}
+
+pd_status pd_adaptive_denoise_patches(const pd_geometry* g, const pd_params* p, const pd_adaptive* a,
+                                      const void* d_in, const double* d_noise_std, const int32_t* d_patch_list,
+                                      int64_t n_selected, void* d_out_acc, float* d_weight_acc, float* d_noise_acc,
+                                      float* d_noise_ctr, int32_t* d_rank_map, int32_t* d_patch_rank,
+                                      float* d_patch_noise, void* d_ws, size_t ws_bytes, void* stream) {
+  g_err.clear();
+  if (!p || p->method != PD_METHOD_ADAPTIVE)
+    return fail(PD_ERR_INVALID, "pd_adaptive_denoise_patches needs method PD_METHOD_ADAPTIVE");
+  if (!a) return fail(PD_ERR_INVALID, "NULL adaptive parameters");
+  if (a->mode < PD_ADAPTIVE_SURE || a->mode > PD_ADAPTIVE_QUT)
+    return fail(PD_ERR_INVALID, "unknown adaptive mode %d", a->mode);
+  if (a->mode == PD_ADAPTIVE_QUT) {
+    if (a->n_gamma < 0 || a->n_gamma > 1) return fail(PD_ERR_INVALID, "QUT takes one fixed gamma or none");
+    if (!(a->qut_level > 0.0)) return fail(PD_ERR_INVALID, "QUT needs a positive Monte-Carlo level");
+  } else if (a->n_gamma < 1 || a->n_gamma > PD_ADAPTIVE_MAX_GAMMA) {
+    return fail(PD_ERR_INVALID, "SURE / GSURE need 1 to %d candidate gammas", PD_ADAPTIVE_MAX_GAMMA);
+  }
+  if (!p->has_prior) return fail(PD_ERR_INVALID, "the adaptive denoiser needs the noise_std map");
+  return denoise_patches_impl(g, p, d_in, d_noise_std, d_patch_list, n_selected, d_out_acc, d_weight_acc,
+                              d_noise_acc, d_noise_ctr, d_rank_map, d_patch_rank, d_patch_noise, d_ws, ws_bytes,
+                              stream, nullptr, a);
 }
 
 // Spatial extents padded to 3 axes (block 1 on padded axes) and frame count.

@@ -559,12 +559,256 @@ __device__ double shrink(int loss, double y, double beta) {
 }
 
 // ---------------------------------------------------------------------------
+// Adaptive trace-norm shrinkage (AdaptiveDenoiser, space_time/lowrank.py:410-636)
+// ---------------------------------------------------------------------------
+// Singular values s (descending), their logs, and si_i = sum_{j != i} 1 / (s_i^2 - s_j^2).
+struct AdSpec {
+  const double* s;
+  const double* ls;
+  const double* si;
+  int nv;
+  double M, T, sigma;
+  bool gsure;
+};
+
+// numpy.maximum(x, 0): NaN propagates
+__device__ __forceinline__ double np_max0(double x) { return x != x ? x : (x > 0.0 ? x : 0.0); }
+
+// _sure_atn_cost (lowrank.py:410-447) at log tau = lt and gamma, in FP64; one
+// warp, every lane returns the same value. d_i = s_i max(1 - (tau/s_i)^gamma, 0);
+// div = sum_i [1 + (gamma-1)(tau/s_i)^gamma](s_i >= tau) + |M - T| d_i / s_i
+// + 2 sum_ij D_ij with D_ij = s_i d_i / (s_i^2 - s_j^2) off the diagonal, so
+// sum_ij D_ij = sum_i s_i d_i si_i; rss = sum_i (d_i - s_i)^2.
+// SURE: sigma^2 (2 div - M T) + rss; GSURE: rss / (1 - div / (M T))^2.
+__device__ double ad_cost(const AdSpec& c, double lt, double gamma) {
+  const int lane = threadIdx.x & 31;
+  const double tau = exp(lt);
+  double dv = 0.0, sd = 0.0, rss = 0.0;
+  for (int k = lane; k < c.nv; k += 32) {
+    const double s = c.s[k];
+    const double r = exp(gamma * (lt - c.ls[k]));  // (tau / s)^gamma
+    const double dh = s * np_max0(1.0 - r);
+    dv += (1.0 + (gamma - 1.0) * r) * (s >= tau ? 1.0 : 0.0) + fabs(c.M - c.T) * dh / s;
+    sd += s * dh * c.si[k];
+    rss += (dh - s) * (dh - s);
+  }
+  dv = warp_sum(dv);
+  sd = warp_sum(sd);
+  rss = warp_sum(rss);
+  const double div = dv + 2.0 * sd;
+  if (c.gsure) {
+    const double q = 1.0 - div / c.M / c.T;
+    return rss / (q * q);
+  }
+  return c.sigma * c.sigma * (2.0 * div - c.M * c.T) + rss;
+}
+
+// Brent's minimisation on [a, b] (golden section with parabolic steps;
+// R. P. Brent, Algorithms for Minimization without Derivatives, 1973, ch. 5),
+// relative tolerance tol. f must return the same value on every lane.
+template <class F>
+__device__ double brent_min(const F& f, double a, double b, double tol) {
+  const double cg = 0.3819660112501051;  // (3 - sqrt 5) / 2
+  double x = a + cg * (b - a), w = x, v = x;
+  double fx = f(x), fw = fx, fv = fx;
+  double d = 0.0, e = 0.0;
+  for (int it = 0; it < 200; ++it) {
+    const double m = 0.5 * (a + b);
+    const double tol1 = tol * fabs(x) + 1e-12, tol2 = 2.0 * tol1;
+    if (fabs(x - m) <= tol2 - 0.5 * (b - a)) break;
+    bool golden = true;
+    if (fabs(e) > tol1) {
+      const double r = (x - w) * (fx - fv);
+      double q = (x - v) * (fx - fw);
+      double pp = (x - v) * q - (x - w) * r;
+      q = 2.0 * (q - r);
+      if (q > 0.0) pp = -pp;
+      else q = -q;
+      const double e_old = e;
+      e = d;
+      if (fabs(pp) < fabs(0.5 * q * e_old) && pp > q * (a - x) && pp < q * (b - x)) {
+        d = pp / q;
+        const double u = x + d;
+        if (u - a < tol2 || b - u < tol2) d = x < m ? tol1 : -tol1;
+        golden = false;
+      }
+    }
+    if (golden) {
+      e = x < m ? b - x : a - x;
+      d = cg * e;
+    }
+    const double u = fabs(d) >= tol1 ? x + d : x + (d > 0.0 ? tol1 : -tol1);
+    const double fu = f(u);
+    if (fu <= fx) {
+      if (u < x) b = x;
+      else a = x;
+      v = w;
+      fv = fw;
+      w = x;
+      fw = fx;
+      x = u;
+      fx = fu;
+    } else {
+      if (u < x) a = u;
+      else b = u;
+      if (fu <= fw || w == x) {
+        v = w;
+        fv = fw;
+        w = u;
+        fw = fu;
+      } else if (fu <= fv || v == x || v == w) {
+        v = u;
+        fv = fu;
+      }
+    }
+  }
+  return x;
+}
+
+// The local minimum of f on [xlo, xhi] that scipy.optimize.minimize (BFGS,
+// forward-difference gradient with step 1.49e-8) heads for from x0: the first
+// line-search trial point of BFGS is x0 - g min(1, 1.01 / |g|) with g the slope
+// at x0; from there the step grows by the golden ratio while the cost keeps
+// falling, and Brent's method refines the minimum inside the bracket. The
+// bounds keep the search where the cost is numerically meaningful.
+template <class F>
+__device__ double ad_minimize(const F& f, double x0, double xlo, double xhi) {
+  x0 = fmin(fmax(x0, xlo), xhi);
+  const double fa0 = f(x0);
+  const double g = (f(x0 + 1.4901161193847656e-08) - fa0) / 1.4901161193847656e-08;
+  if (!(fabs(g) > 0.0)) return x0;  // flat or NaN
+  double a = x0, fa = fa0;
+  double b = fmin(fmax(x0 - g * fmin(1.0, 1.01 / fabs(g)), xlo), xhi);
+  if (b == a) return x0;
+  double fb = f(b);
+  double lo, hi;
+  if (fb < fa) {
+    double c = fmin(fmax(b + 1.618033988749895 * (b - a), xlo), xhi), fc = f(c);
+    for (int it = 0; it < 60 && fc < fb && c != b && xlo < c && c < xhi; ++it) {
+      a = b;
+      fa = fb;
+      b = c;
+      fb = fc;
+      c = fmin(fmax(b + 1.618033988749895 * (b - a), xlo), xhi);
+      fc = f(c);
+    }
+    lo = fmin(a, c);
+    hi = fmax(a, c);
+  } else {
+    lo = fmin(a, b);
+    hi = fmax(a, b);
+  }
+  return brent_min(f, lo, hi, 1e-10);
+}
+
+// The adaptive rule for one patch (the caller's whole CTA): the full spectrum,
+// the (G)SURE minimisation and the shrinkage coefficients. Compiled only into
+// k_eig's ADAPT instantiation, so that its FP64 search leaves the other
+// methods' kernels as they are. scratch: 3 n doubles of shared memory.
+__device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adaptive& ad, const PatchWork& w, int p,
+                                              int n, const float* d,
+                                           const float* e2, const TriInfo& ti, int* idx, float* lam, int* aidx,
+                                           float* alam, float* acoef, double* scratch, double tscale, double M,
+                                           double pt, int* s_act) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // the whole spectrum: singular values s = sqrt(eigenvalue) in numpy.svd's
+  // (descending) order, min(M, n) of them
+  for (int i = tid; i < n; i += EIG_THREADS) idx[i] = i;
+  __syncthreads();
+  cta_eigs(d, e2, n, ti, idx, lam, n);
+  const int nv = ep.rows < n ? ep.rows : n;
+  double* sv = scratch;
+  double* lsv = sv + n;
+  double* si = lsv + n;
+  for (int k = tid; k < nv; k += EIG_THREADS) {
+    sv[k] = sqrt(fmax((double)lam[n - 1 - k] * tscale, 0.0));
+    lsv[k] = log(sv[k]);
+  }
+  __syncthreads();
+  for (int k = tid; k < nv; k += EIG_THREADS) {
+    const double a2 = sv[k] * sv[k];
+    double acc = 0.0;
+    for (int q = 0; q < nv; ++q)
+      if (q != k) acc += 1.0 / (a2 - sv[q] * sv[q]);
+    si[k] = acc;
+  }
+  __syncthreads();
+  __shared__ double s_cost[PD_ADAPTIVE_MAX_GAMMA], s_x[PD_ADAPTIVE_MAX_GAMMA];
+  __shared__ double s_gamma, s_lt;
+  const AdSpec c{sv, lsv, si, nv, M, pt, sqrt(w.prior[p]), ad.mode == PD_ADAPTIVE_GSURE};
+  if (ad.mode == PD_ADAPTIVE_QUT) {
+    // tau = stdest * level (lowrank.py:464-475); gamma fixed, or exp(x) + 1 with
+    // x minimising the cost from 0 (lowrank.py:477-492)
+    const double lt = log(c.sigma * ad.qut_level);
+    if (warp == 0) {
+      double gq = ad.n_gamma >= 1 ? ad.gamma[0] : 0.0;
+      if (ad.n_gamma < 1)
+        gq = exp(ad_minimize([&](double x) { return ad_cost(c, lt, exp(x) + 1.0); }, 0.0, -700.0, 700.0)) + 1.0;
+      if (lane == 0) {
+        s_gamma = gq;
+        s_lt = lt;
+      }
+    }
+  } else {
+    // every candidate gamma: log tau from log(median s) (or tau0) by the search,
+    // the lowest cost wins, the first on ties (lowrank.py:497-533); a warp per
+    // candidate. log tau stays within 10 of the log spectrum: far below the
+    // smallest singular value every d equals s to rounding and the GSURE cost
+    // is 0/0 (rss and 1 - div/(M T) both vanish with gamma = 1).
+    const double xlo = lsv[nv - 1] - 10.0, xhi = lsv[0] + 10.0;
+    double x0 = ad.tau0;
+    if (!ad.has_tau0) x0 = log((nv & 1) ? sv[nv / 2] : 0.5 * (sv[nv / 2 - 1] + sv[nv / 2]));
+    for (int q = warp; q < ad.n_gamma; q += EIG_NW) {
+      const double gq = ad.gamma[q];
+      const double x = ad_minimize([&](double xx) { return ad_cost(c, xx, gq); }, x0, xlo, xhi);
+      const double cost = ad_cost(c, x, gq);
+      if (lane == 0) {
+        s_cost[q] = cost;
+        s_x[q] = x;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int bq = 0;  // no finite cost at all (the reference fails there): the first candidate
+      double best = INFINITY;
+      for (int q = 0; q < ad.n_gamma; ++q)
+        if (s_cost[q] < best) {
+          best = s_cost[q];
+          bq = q;
+        }
+      s_gamma = ad.gamma[bq];
+      s_lt = s_x[bq];
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    // _atn_shrink (lowrank.py:459-461); maxidx = last nonzero + 1 (lowrank.py:628-635)
+    const double gq = s_gamma, lt = s_lt;
+    int maxidx = 0;
+    for (int k = 0; k < nv; ++k) {
+      const double dh = sv[k] * np_max0(1.0 - exp(gq * (lt - lsv[k])));
+      if (dh != 0.0) maxidx = k + 1;  // NaN counts as nonzero, as in numpy
+      acoef[k] = (float)(dh / sv[k]);
+    }
+    for (int k = 0; k < maxidx; ++k) {
+      aidx[k] = n - 1 - k;
+      alam[k] = lam[n - 1 - k];
+    }
+    w.rank[p] = maxidx;
+    w.noise[p] = nanf("");
+    *s_act = maxidx;
+  }
+  __syncthreads();}
+
+// ---------------------------------------------------------------------------
 // The kernel
 // ---------------------------------------------------------------------------
-template <bool CPLX, int NS>
+template <bool CPLX, int NS, bool ADAPT>
+// ADAPT: with the adaptive rule (PD_METHOD_ADAPTIVE launches only).
 // in_smem: bit 0 = the packed matrix lives in shared memory, bit 1 = the
 // Lanczos basis of the top-1 mode does too (after the layout's end).
-__global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, PatchWork w, int in_smem) {
+__global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, PatchWork w, int in_smem,
+                                                       pd_adaptive ad) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ __align__(16) unsigned char sm[];
   const EigLayout L = eig_layout(CPLX, n, (in_smem & 1) != 0);
@@ -645,7 +889,10 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
   const double M = (double)ep.rows, pt = (double)ep.cols;
 
   // ---------------------------------------------------------------- decisions
-  if (ep.method == PD_METHOD_MPPCA || ep.method == PD_METHOD_HYBRID) {
+  if (ADAPT && ep.method == PD_METHOD_ADAPTIVE) {  // compiled into the ADAPT instantiation only
+    adaptive_rule(ep, ad, w, p, n, d, e2, ti, idx, lam, aidx, alam, acoef, reinterpret_cast<double*>(pw), tscale, M,
+                  pt, &s_act);
+  } else if (ep.method == PD_METHOD_MPPCA || ep.method == PD_METHOD_HYBRID) {
     const int ne = n < 10 ? n : 10;
     if (tid < ne) idx[tid] = n - ne + tid;
     __syncthreads();
@@ -1014,7 +1261,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_top1(int n, PatchWork w) {
 }
 
 template <bool CPLX, int NS>
-static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
+static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s, const pd_adaptive* ad) {
   bool in_smem;
   size_t smem = eig_smem_bytes(CPLX, n, &in_smem);
   int flags = in_smem ? 1 : 0;
@@ -1025,22 +1272,27 @@ static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaSt
       flags |= 2;
     }
   }
-  cudaError_t err = cudaFuncSetAttribute(k_eig<CPLX, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto kern = ep.method == PD_METHOD_ADAPTIVE ? k_eig<CPLX, NS, true> : k_eig<CPLX, NS, false>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  PD_TIMED(ep.method == EIG_MODE_TOP1 ? "eig_mc" : "eig", s, k_eig<CPLX, NS><<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, flags));
+  pd_adaptive a{};
+  if (ad) a = *ad;
+  PD_TIMED(ep.method == EIG_MODE_TOP1 ? "eig_mc" : "eig", s, kern<<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, flags, a));
   return cudaGetLastError();
 }
 
 template <bool CPLX>
-static cudaError_t eig_dispatch(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
-  if (n <= 64) return eig_ns<CPLX, 2>(n, ep, w, s);
-  if (n <= 128) return eig_ns<CPLX, 4>(n, ep, w, s);
-  if (n <= 224) return eig_ns<CPLX, 7>(n, ep, w, s);
-  if (n <= 320) return eig_ns<CPLX, 10>(n, ep, w, s);
-  return eig_ns<CPLX, 14>(n, ep, w, s);
+static cudaError_t eig_dispatch(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s,
+                                const pd_adaptive* ad) {
+  if (n <= 64) return eig_ns<CPLX, 2>(n, ep, w, s, ad);
+  if (n <= 128) return eig_ns<CPLX, 4>(n, ep, w, s, ad);
+  if (n <= 224) return eig_ns<CPLX, 7>(n, ep, w, s, ad);
+  if (n <= 320) return eig_ns<CPLX, 10>(n, ep, w, s, ad);
+  return eig_ns<CPLX, 14>(n, ep, w, s, ad);
 }
 
-cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
+cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s,
+                       const pd_adaptive* ad) {
   if (!cplx && ep.method == EIG_MODE_TOP1) {
     const size_t smem = top1_smem_bytes(n);
     if (smem <= EIG_SMEM_LIMIT) {
@@ -1050,7 +1302,7 @@ cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w
       return cudaGetLastError();
     }
   }
-  return cplx ? eig_dispatch<true>(n, ep, w, s) : eig_dispatch<false>(n, ep, w, s);
+  return cplx ? eig_dispatch<true>(n, ep, w, s, ad) : eig_dispatch<false>(n, ep, w, s, ad);
 }
 
 }  // namespace pd

@@ -52,9 +52,10 @@ __global__ void __launch_bounds__(MEAN_THREADS) k_patch_mean(Geo g, const typena
   }
 }
 
-// Hybrid: varest = mean(noise_std^2) over the patch; optimal: sigma = mean(|noise_std|).
-// (space_time/lowrank.py:106 and :389; the maps are constant along time so the
-// 4D patch mean equals the spatial one.)
+// Hybrid: varest = mean(noise_std^2) over the patch; optimal: sigma = mean(|noise_std|);
+// adaptive: mean(noise_std^2), whose root is the patch's stdest.
+// (space_time/lowrank.py:106, :389 and :617; the maps are constant along time so
+// the 4D patch mean equals the spatial one.)
 __global__ void k_prior(Geo g, int method, const double* __restrict__ ns, PatchWork w) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -65,7 +66,7 @@ __global__ void k_prior(Geo g, int method, const double* __restrict__ ns, PatchW
     double s = 0.0;
     for (int r = lane; r < g.rows; r += 32) {
       const double v = ns[row_voxel(g, o, r)];
-      s += (method == PD_METHOD_HYBRID) ? v * v : sqrt(v * v);
+      s += (method == PD_METHOD_HYBRID || method == PD_METHOD_ADAPTIVE) ? v * v : sqrt(v * v);
     }
     s = warp_sum(s);
     if (lane == 0) w.prior[p] = s / g.rows;

@@ -60,7 +60,8 @@ struct EigParams {
   const double* d_threshold;  // raw / NORDIC: read the threshold here when not NULL
 };
 constexpr int EIG_MODE_TOP1 = 100;
-cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s);
+cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s,
+                       const pd_adaptive* ad = nullptr);
 size_t eig_smem_bytes(bool cplx, int n, bool* in_smem);
 
 // pd_synth.cu

@@ -55,7 +55,8 @@ def optimal_thresholding(input_data, patch_shape, patch_overlap, mask=None, mask
 
 def adaptive_thresholding(input_data, patch_shape, patch_overlap, mask=None, mask_threshold=50,
                           recombination="weighted", method="SURE", nbsim=500, tau0=None, gamma0=None,
-                          noise_std=1.0, progbar=None):
-    """Adaptive shrinkage (denoise.py:285-347): not on the GPU path, raises NotImplementedError."""
-    den = AdaptiveDenoiser(patch_shape, patch_overlap, recombination=recombination, method=method, nbsim=nbsim)
+                          noise_std=1.0, progbar=None, *, precision="fp32"):
+    """Adaptive trace-norm shrinkage, SURE / GSURE / QUT (denoise.py:285-347)."""
+    den = AdaptiveDenoiser(patch_shape, patch_overlap, recombination=recombination, method=method, nbsim=nbsim,
+                           precision=precision)
     return den.denoise(input_data, mask, mask_threshold, tau0, noise_std, gamma0, progbar=progbar)

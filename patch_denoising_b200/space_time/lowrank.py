@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .. import _engine
+from .. import _engine, _lib
 from .base import BaseSpaceTimeDenoiser, _is_float_scalar
 
 
@@ -149,21 +149,63 @@ class OptimalSVDDenoiser(BaseSpaceTimeDenoiser):
 
 
 class AdaptiveDenoiser(BaseSpaceTimeDenoiser):
-    """Adaptive trace-norm shrinkage (space_time/lowrank.py:536-636).
+    """Adaptive trace-norm shrinkage d = s max(1 - (tau/s)^gamma, 0) (space_time/lowrank.py:536-636).
 
-    Not part of the GPU path of this package: ``denoise`` raises.
+    ``method`` "sure" / "gsure": for every candidate in ``gamma0`` (an iterable,
+    as in the reference) log tau minimises the SURE / GSURE cost from ``tau0``
+    (default log of the median singular value); the lowest cost wins. "qut":
+    tau = stdest x the (1 - 1/sqrt(log max(M, T)))-quantile of the largest
+    singular value of ``nbsim`` Gaussian M x T draws (one set per call, seeded
+    from NumPy's global generator, ``qut_level_``; ``qut_level`` supplies it);
+    gamma is ``gamma0`` when it is a float, else minimises the cost. stdest is
+    sqrt(mean noise_std^2) over the patch. The cost minimisation runs on the
+    device (bracketing line search + Brent) in place of scipy's BFGS.
     """
 
+    _method = "adaptive"
     _SUPPORTED_METHOD = ["sure", "qut", "gsure"]
 
-    def __init__(self, patch_shape, patch_overlap, method="SURE", recombination="weighted", nbsim=500):
-        super().__init__(patch_shape, patch_overlap, recombination)
+    def __init__(self, patch_shape, patch_overlap, method="SURE", recombination="weighted", nbsim=500, *,
+                 precision="fp32"):
+        super().__init__(patch_shape, patch_overlap, recombination, precision=precision)
         if method.lower() not in self._SUPPORTED_METHOD:
             raise ValueError(f"Unsupported method: '{method}', use any of {self._SUPPORTED_METHOD}")
         self.input_denoising_kwargs["method"] = method.lower()
         self.input_denoising_kwargs["nbsim"] = nbsim
+        self.qut_level_ = None
 
     def denoise(self, input_data, mask=None, mask_threshold=50, tau0=None, noise_std=None, gamma0=None,
-                progbar=None):
-        """Not implemented on the GPU path."""
-        raise NotImplementedError("AdaptiveDenoiser (SURE/GSURE/QUT) has no GPU implementation in this package")
+                progbar=None, qut_level=None):
+        """Denoise with adaptive shrinkage; ``noise_std`` (float or spatial map) is required."""
+        method = self.input_denoising_kwargs["method"]
+        if noise_std is None:  # the reference squares it
+            raise TypeError("unsupported operand type(s) for ** or pow(): 'NoneType' and 'int'")
+        self.input_denoising_kwargs["gamma0"] = gamma0
+        self.input_denoising_kwargs["tau0"] = tau0
+        self.input_denoising_kwargs["noise_std"] = noise_std
+        ad = {"mode": method}
+        if method == "qut":
+            ad["gamma"] = [float(gamma0)] if isinstance(gamma0, (float, np.floating)) else []
+            self._qut_seed = None if qut_level is not None else int(np.random.randint(0, 2**62))
+            self.qut_level_ = None if qut_level is None else float(qut_level)
+        else:
+            gam = [float(g) for g in gamma0]  # TypeError for None or a scalar, as the reference's loop
+            if not gam:
+                raise UnboundLocalError("no candidate gamma: gamma0 is empty")
+            if len(gam) > _lib.ADAPTIVE_MAX_GAMMA:
+                raise NotImplementedError(f"at most {_lib.ADAPTIVE_MAX_GAMMA} candidate gammas")
+            ad["gamma"] = gam
+            ad["tau0"] = None if tau0 is None else float(np.asarray(tau0).reshape(-1)[0])
+        self._adaptive = ad
+        return self._denoise(input_data, mask, mask_threshold, progbar)
+
+    def _method_args(self, data_shape, p_s, device):
+        ad = dict(self._adaptive)
+        if ad["mode"] == "qut":
+            if self.qut_level_ is None:
+                rows, cols = int(np.prod(p_s[:-1])), int(p_s[-1])
+                self.qut_level_ = _engine.adaptive_qut_level(rows, cols, int(self.input_denoising_kwargs["nbsim"]),
+                                                             self._qut_seed, device, self.precision)
+            ad["qut_level"] = self.qut_level_
+        ns = self.input_denoising_kwargs["noise_std"]
+        return {"noise_std": self._spatial_map(ns, data_shape, device), "adaptive": ad}

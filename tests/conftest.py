@@ -65,6 +65,36 @@ def load_golden(name):
     return arrays, call
 
 
+def adaptive_golden_names():
+    return sorted(p.stem for p in (GOLDEN / "adaptive").glob("*.npz"))
+
+
+def load_adaptive_golden(name):
+    """(arrays, call) of an adaptive fixture; ``call`` holds the oracle's keyword
+    arguments (``adaptive_method``, ``gamma0``, ``tau0``, ``nbsim``, ``seed``)."""
+    z = np.load(GOLDEN / "adaptive" / f"{name}.npz", allow_pickle=False)
+    arrays = {k: z[k] for k in z.files if not k.startswith("meta_")}
+    meta = {k[5:]: z[k] for k in z.files if k.startswith("meta_")}
+    ns = arrays["noise_std"]
+    call = dict(
+        method="adaptive",
+        patch_shape=int(meta["patch"]),
+        patch_overlap=int(meta["overlap"]),
+        recombination=str(meta["recombination"]),
+        adaptive_method=str(meta["method"]),
+        noise_std=float(ns) if ns.ndim == 0 else ns,
+        nbsim=int(meta["nbsim"]),
+        gamma0=None,
+        tau0=float(meta["tau0"]) if "tau0" in meta else None,
+    )
+    if "gamma0" in arrays:
+        g = arrays["gamma0"]
+        call["gamma0"] = float(g) if g.ndim == 0 else g
+    if "seed" in meta:
+        call["seed"] = int(meta["seed"])
+    return arrays, call
+
+
 @pytest.fixture(scope="session")
 def golden():
     return {n: load_golden(n) for n in golden_names()}

@@ -1,7 +1,7 @@
 """The reference's own acceptance checks (its tests/test_denoiser.py strategy),
 run through this package on the reference's phantom fixture: every method and
-recombination must lower the residual noise level, and NORDIC must reject a
-non-numeric noise level."""
+recombination (the adaptive SURE / GSURE / QUT shrinkage included) must lower
+the residual noise level, and NORDIC must reject a non-numeric noise level."""
 
 from __future__ import annotations
 
@@ -74,9 +74,20 @@ def test_nordic_rejects_a_non_numeric_noise_level():
         nordic(NOISY, patch_shape=6, patch_overlap=5, noise_std="not_a_float_or_array")
 
 
-@pytest.mark.parametrize("method, gamma", [("qut", None), ("gsure", np.linspace(1, 5, 10))])
-def test_adaptive_is_not_built(method, gamma):
-    """Adaptive SURE / QUT shrinkage is outside this package's scope: it says so."""
-    with pytest.raises(NotImplementedError):
-        adaptive_thresholding(NOISY, patch_shape=10, patch_overlap=0, method=method, noise_std=2 * G_MAP,
+@pytest.mark.parametrize("recombination", ["weighted", "average"])
+@pytest.mark.parametrize(
+    "method, gamma", [("qut", None), ("gsure", np.linspace(1, 5, 10)), ("sure", np.linspace(1, 5, 10))]
+)
+def test_adaptive_lowers_noise(recombination, method, gamma):
+    """The reference's adaptive check: patch 10, no overlap, noise map 2 g, nbsim 500."""
+    np.random.seed(3)
+    _lowers_noise(adaptive_thresholding(NOISY, patch_shape=10, patch_overlap=0, recombination=recombination,
+                                        method=method, noise_std=2 * G_MAP, gamma0=gamma, nbsim=500))
+
+
+@pytest.mark.parametrize("gamma", [None, 2.0])
+def test_adaptive_sure_needs_a_gamma_list(gamma):
+    """As the reference's loop over gamma0: a missing or scalar gamma0 is a TypeError."""
+    with pytest.raises(TypeError):
+        adaptive_thresholding(NOISY, patch_shape=10, patch_overlap=0, method="SURE", noise_std=2 * G_MAP,
                               gamma0=gamma)

@@ -170,3 +170,18 @@ def test_nonfinite_patch_word_raises_value_error():
     with pytest.raises(ValueError, match="infs or NaNs"):
         _engine.check_device_errors()
     assert not _engine._pending_errors
+
+
+def test_adaptive_argument_errors_match_the_reference():
+    """Raised before any device work, as the reference raises them."""
+    from patch_denoising_b200.space_time import AdaptiveDenoiser
+
+    with pytest.raises(ValueError):
+        AdaptiveDenoiser(4, 2, method="lasso")
+    x = np.zeros((8, 8, 8, 10), dtype=np.float32)
+    with pytest.raises(TypeError):  # noise_std ** 2 with None
+        AdaptiveDenoiser(4, 2, method="sure").denoise(x, gamma0=[1.0])
+    with pytest.raises(TypeError):  # for g in gamma0 with None / a scalar
+        AdaptiveDenoiser(4, 2, method="sure").denoise(x, noise_std=1.0, gamma0=None)
+    with pytest.raises(TypeError):
+        AdaptiveDenoiser(4, 2, method="gsure").denoise(x, noise_std=1.0, gamma0=2.0)
