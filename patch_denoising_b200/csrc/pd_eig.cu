@@ -1095,13 +1095,37 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
         continue;
       }
       float* za = vbase + (int64_t)a * n2;
-      for (int b = cstart; b < a; ++b) {
-        const float* zb = vbase + (int64_t)b * n2;
-        float part = 0.f;
-        for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * zb[i];
-        const float dt = bsum_f(part);
-        for (int i = tid; i < n; i += EIG_THREADS) za[i] -= dt * zb[i];
-        __syncthreads();
+      if constexpr (ADAPT) {
+        // Adaptive shrinkage keeps whole noise bulks, one cluster of up to n
+        // vectors: classical Gram-Schmidt against the cluster, twice. The
+        // projections of a pass are independent (a warp per earlier vector),
+        // so a vector costs four barriers instead of three per earlier vector.
+        float* dots = reinterpret_cast<float*>(idx);  // free after the decisions
+        for (int pass = 0; pass < 2; ++pass) {
+          for (int b = cstart + warp; b < a; b += EIG_NW) {
+            const float* zb = vbase + (int64_t)b * n2;
+            float dp = 0.f;
+            for (int i = lane; i < n; i += 32) dp += za[i] * zb[i];
+            dp = warp_sum(dp);
+            if (lane == 0) dots[b - cstart] = dp;
+          }
+          __syncthreads();
+          for (int i = tid; i < n; i += EIG_THREADS) {
+            float v = za[i];
+            for (int b = cstart; b < a; ++b) v -= dots[b - cstart] * vbase[(int64_t)b * n2 + i];
+            za[i] = v;
+          }
+          __syncthreads();
+        }
+      } else {
+        for (int b = cstart; b < a; ++b) {
+          const float* zb = vbase + (int64_t)b * n2;
+          float part = 0.f;
+          for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * zb[i];
+          const float dt = bsum_f(part);
+          for (int i = tid; i < n; i += EIG_THREADS) za[i] -= dt * zb[i];
+          __syncthreads();
+        }
       }
       float part = 0.f;
       for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * za[i];
