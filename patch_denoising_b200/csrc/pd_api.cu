@@ -389,6 +389,7 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
     sa.patch_rank = d_patch_rank;
     sa.patch_noise = d_patch_noise;
     sa.list_offset = off;
+    sa.wide = p->method == PD_METHOD_ADAPTIVE ? 1 : 0;
     launch_synth(G, cplx, d_in, w, sa, s);
     PD_TRY(cuda_check(cudaGetLastError(), "pd_denoise_patches launch"));
   }

@@ -148,43 +148,6 @@ template <>
 __device__ __forceinline__ cf shfl_idx<cf>(cf v, int src) {
   return cf{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
 }
-template <class T>
-__device__ __forceinline__ T shfl_x(T v, int m);
-template <>
-__device__ __forceinline__ float shfl_x<float>(float v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
-template <>
-__device__ __forceinline__ cf shfl_x<cf>(cf v, int m) {
-  return cf{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
-}
-
-// dp[q] (q < 8) summed over the warp; lane returns (column slot, total) with
-// slot = 4*b16 + 2*b8 + b4 valid on lanes with (lane & 3) == 0.
-template <class T>
-__device__ __forceinline__ T reduce_scatter8(const T dp[8], int lane, int* slot) {
-  const bool b16 = lane & 16, b8 = lane & 8, b4 = lane & 4;
-  T k4[4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const T snd = b16 ? dp[q] : dp[q + 4];
-    const T rcv = shfl_x(snd, 16);
-    k4[q] = (b16 ? dp[q + 4] : dp[q]) + rcv;
-  }
-  T k2[2];
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    const T snd = b8 ? k4[q] : k4[q + 2];
-    const T rcv = shfl_x(snd, 8);
-    k2[q] = (b8 ? k4[q + 2] : k4[q]) + rcv;
-  }
-  const T snd = b4 ? k2[0] : k2[1];
-  const T rcv = shfl_x(snd, 4);
-  T k1 = (b4 ? k2[1] : k2[0]) + rcv;
-  k1 = k1 + shfl_x(k1, 2);
-  k1 = k1 + shfl_x(k1, 1);
-  *slot = (b16 ? 4 : 0) + (b8 ? 2 : 0) + (b4 ? 1 : 0);
-  return k1;
-}
-
 template <bool CPLX, int NS>
 __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float* e, typename Elem<CPLX>::T* tau,
                                typename Elem<CPLX>::T* vb, typename Elem<CPLX>::T* wb,

@@ -75,6 +75,7 @@ struct SynthArgs {
   int32_t* patch_rank;  // per listed patch (global list position)
   float* patch_noise;
   int64_t list_offset;  // position of the chunk inside the full list
+  int wide;             // high ranks expected (adaptive shrinkage): the grouped-reduction kernel
 };
 void launch_synth(const Geo& g, bool cplx, const void* in, const PatchWork& w, const SynthArgs& a,
                   cudaStream_t s);

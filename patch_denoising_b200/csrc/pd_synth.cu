@@ -23,7 +23,9 @@ __device__ __forceinline__ void acc_add(cf* p, cf v) {
   atomicAdd(reinterpret_cast<float2*>(p), make_float2(v.x, v.y));
 }
 
-template <bool CPLX, int NS, int R>
+// WIDE: with the grouped reduction for ranks above 8 (adaptive launches only;
+// its registers would cost the low-rank methods occupancy).
+template <bool CPLX, int NS, int R, bool WIDE>
 __global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
                                                        PatchWork w, SynthArgs sa, int ysplit) {
   using T = typename Elem<CPLX>::T;
@@ -88,7 +90,37 @@ __global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Ele
           const int t = lane + 32 * s;
           x[q][s] = (ok[q] && t < n) ? in[base[q] + t] - smean[t] : zero<T>();
         }
-      for (int a = 0; a < act; ++a) {
+      int a = 0;
+      if (WIDE && act > 8) {
+        // a high rank (the adaptive shrinkage keeps whole spectra): the row
+        // sums of eight components leave in one reduce-scatter butterfly
+        // instead of eight warp sums
+        for (; a + 8 <= act; a += 8) {
+          T pg[R][8];
+#pragma unroll
+          for (int q = 0; q < R; ++q)
+#pragma unroll
+            for (int g = 0; g < 8; ++g) pg[q][g] = zero<T>();
+#pragma unroll
+          for (int g = 0; g < 8; ++g)
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+              const int t = lane + 32 * s;
+              if (t < n) {
+                const T v = vat(a + g, t);
+#pragma unroll
+                for (int q = 0; q < R; ++q) pg[q][g] = pg[q][g] + mul(x[q][s], v);
+              }
+            }
+#pragma unroll
+          for (int q = 0; q < R; ++q) {
+            int slot;
+            const T tot = reduce_scatter8<T>(pg[q], lane, &slot);
+            if ((lane & 3) == 0) yw[q * n + a + slot] = tot * scoef[a + slot];
+          }
+        }
+      }
+      for (; a < act; ++a) {
         T pa[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) pa[q] = zero<T>();
@@ -175,13 +207,14 @@ static void synth_ns(const Geo& g, const void* in, const PatchWork& w, const Syn
   constexpr int R = CPLX ? 2 : 4;
   const int n = g.cols;
   const size_t smem = sizeof(T) * ((size_t)SYN_NW * R * n + n) + sizeof(float) * n + 16;
-  cudaFuncSetAttribute(k_synth<CPLX, NS, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto kern = a.wide ? k_synth<CPLX, NS, R, true> : k_synth<CPLX, NS, R, false>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int rows_per_block = SYN_NW * R;
   int ysplit = (g.rows + rows_per_block - 1) / rows_per_block;
   if (ysplit > 8) ysplit = 8;
   if (a.recombination == PD_RECOMB_CENTER) ysplit = 1;
   const unsigned grid = (unsigned)((int64_t)w.count * ysplit);
-  PD_TIMED("synth_scatter", s, k_synth<CPLX, NS, R><<<grid, SYN_THREADS, smem, s>>>(g, (const T*)in, w, a, ysplit));
+  PD_TIMED("synth_scatter", s, kern<<<grid, SYN_THREADS, smem, s>>>(g, (const T*)in, w, a, ysplit));
 }
 
 template <bool CPLX>
