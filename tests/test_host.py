@@ -185,3 +185,42 @@ def test_adaptive_argument_errors_match_the_reference():
         AdaptiveDenoiser(4, 2, method="sure").denoise(x, noise_std=1.0, gamma0=None)
     with pytest.raises(TypeError):
         AdaptiveDenoiser(4, 2, method="gsure").denoise(x, noise_std=1.0, gamma0=2.0)
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """pd_geometry, pd_params and pd_adaptive: the ctypes mirrors have the C layout
+    (size and every field offset), checked by compiling the header with the C compiler."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"pd_geometry": _lib.Geometry, "pd_params": _lib.Params, "pd_adaptive": _lib.Adaptive}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "patch_denoise_b200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(line.split()[:2]): int(line.split()[2]) for line in out if line}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for field, _ in py._fields_:
+            assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
+
+
+def test_adaptive_record_from_the_denoiser_settings():
+    """The pd_adaptive record that pd_adaptive_denoise_patches receives."""
+    ad = _engine._adaptive_struct({"mode": "gsure", "gamma": [1.0, 2.5, 4.0], "tau0": None})
+    assert (ad.mode, ad.n_gamma, ad.has_tau0) == (_lib.ADAPTIVE_MODE["gsure"], 3, 0)
+    assert list(ad.gamma[:3]) == [1.0, 2.5, 4.0]
+    ad = _engine._adaptive_struct({"mode": "sure", "gamma": [2.0], "tau0": 1.75})
+    assert (ad.has_tau0, ad.tau0) == (1, 1.75)
+    ad = _engine._adaptive_struct({"mode": "qut", "gamma": [], "qut_level": 12.5})
+    assert (ad.mode, ad.n_gamma, ad.qut_level) == (_lib.ADAPTIVE_MODE["qut"], 0, 12.5)
