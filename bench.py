@@ -300,7 +300,7 @@ def ours_arm(args, rank, world):
     # per-kernel CUDA-event split from a second, instrumented run (events around
     # every launch add small gaps, so `value` comes from the run above)
     _, kern, _ = timed(precision, prof=True)
-    # plain FP32 kernels on the same workload (the north-star comparison)
+    # plain FP32 kernels on the same workload (the metric's comparison: chosen vs plain FP32)
     ms_fp32 = ms if precision == "fp32" else timed("fp32")[0]
 
     # accuracy of the chosen kernels against the plain FP32 ones at the same Monte-Carlo level
