@@ -513,6 +513,11 @@ pd_status pd_adaptive_qut_level(int64_t rows, int64_t cols, int32_t n_sim, uint6
   g_err.clear();
   if (!out) return fail(PD_ERR_INVALID, "NULL output");
   if (n_sim < 1) return fail(PD_ERR_INVALID, "nbsim must be at least 1");
+  if (rows < 1 || cols < 1) return fail(PD_ERR_INVALID, "empty Monte-Carlo problem");
+  // the quantile's probability; numpy.quantile rejects it outside [0, 1]
+  // (max(rows, cols) < 3), as the reference then fails
+  const double q = 1.0 - 1.0 / sqrt(log((double)std::max(rows, cols)));
+  if (!(q >= 0.0 && q <= 1.0)) return fail(PD_ERR_INVALID, "Quantiles must be in the range [0, 1]");
   cudaStream_t s = (cudaStream_t)stream;
   PatchWork w;
   PD_TRY(mc_launch(rows, cols, n_sim, seed, precision, d_ws, ws_bytes, s, &w));
@@ -527,7 +532,6 @@ pd_status pd_adaptive_qut_level(int64_t rows, int64_t cols, int32_t n_sim, uint6
   // v[floor h] + (h - floor h) (v[floor h + 1] - v[floor h])
   for (auto& v : lam) v = sqrt(fmax(v, 0.0));
   std::sort(lam.begin(), lam.end());
-  const double q = 1.0 - 1.0 / sqrt(log((double)std::max(rows, cols)));
   const double h = (double)(n_sim - 1) * q;
   const int64_t lo = std::min<int64_t>(std::max<int64_t>((int64_t)floor(h), 0), n_sim - 1);
   const int64_t hi = std::min<int64_t>(lo + 1, n_sim - 1);

@@ -224,3 +224,13 @@ def test_adaptive_record_from_the_denoiser_settings():
     assert (ad.has_tau0, ad.tau0) == (1, 1.75)
     ad = _engine._adaptive_struct({"mode": "qut", "gamma": [], "qut_level": 12.5})
     assert (ad.mode, ad.n_gamma, ad.qut_level) == (_lib.ADAPTIVE_MODE["qut"], 0, 12.5)
+
+
+def test_qut_level_rejects_a_quantile_outside_0_1():
+    """max(M, T) < 3 puts the QUT probability 1 - 1/sqrt(log max(M, T)) below 0,
+    which numpy.quantile (and so the reference) rejects; checked before any device work."""
+    lib = _lib.load()
+    out = ctypes.c_double()
+    st = lib.pd_adaptive_qut_level(2, 2, 10, ctypes.c_uint64(1), 0, ctypes.byref(out), None, 0, None)
+    assert st == _lib.PD_ERR_INVALID
+    assert b"Quantiles must be in the range" in lib.pd_last_error()
