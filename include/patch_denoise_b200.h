@@ -229,14 +229,25 @@ pd_status pd_adaptive_denoise_patches(const pd_geometry* g, const pd_params* p, 
  * acceptable. The scratch is a static 32 MiB device array inside the library
  * that every GPU loading the library keeps until exit. Patches are processed
  * in chunks that fit it. A geometry whose single-patch scratch exceeds 32 MiB
- * returns PD_ERR_WORKSPACE. The first call on a device looks up the array's
- * device address; make that call before any stream capture. All calls share the
- * array, so calls that overlap on the GPU (other streams or host threads) race.
+ * returns PD_ERR_WORKSPACE. Every call looks up the array's device address on
+ * the current device; the first call on a device also loads the library's
+ * device code there, so make it before any stream capture. Read the device
+ * error word (NaN / inf samples, timed-out waits) with pd_noalloc_check. All
+ * calls share the array, so calls that overlap on the GPU (other streams or
+ * host threads) race.
  * Arguments are those of pd_denoise_patches minus the workspace. */
 pd_status pd_denoise_patches_noalloc(const pd_geometry* g, const pd_params* p, const void* d_in,
                                      const double* d_noise_std, const int32_t* d_patch_list, int64_t n_selected,
                                      void* d_out_acc, float* d_weight_acc, float* d_noise_acc, float* d_noise_ctr,
                                      int32_t* d_rank_map, int32_t* d_patch_rank, float* d_patch_noise, void* stream);
+
+/* Companion of pd_denoise_patches_noalloc, with no counterpart in the reference:
+ * the caller of the no-allocation entry point has no workspace pointer to hand
+ * to pd_workspace_check, because its scratch (and the device error word at its
+ * start) is the library's static array. This synchronises the stream and reads
+ * that word: PD_ERR_INVALID if a processed patch held a NaN or infinite sample,
+ * PD_ERR_CUDA if a bounded device-side wait timed out, PD_OK otherwise. */
+pd_status pd_noalloc_check(void* stream);
 
 /* Scratch bytes pd_estimate_noise needs (shape as for pd_estimate_noise). */
 pd_status pd_estimate_noise_workspace_size(int32_t ndim, const int64_t* shape, int32_t is_complex, size_t* bytes);

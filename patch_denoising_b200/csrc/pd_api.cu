@@ -364,6 +364,7 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
   ep.threshold = p->threshold;
   ep.mp_median = p->mp_median;
   ep.d_threshold = d_thr;
+  ep.only_unfinished = 0;
   PD_TRY(cuda_check(cudaMemsetAsync(d_ws, 0, sizeof(int), s), "clear error word"));
   for (int64_t off = 0; off < n_selected; off += chunk) {
     const int cnt = (int)std::min<int64_t>(chunk, n_selected - off);
@@ -378,7 +379,15 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
       PD_TRY(cuda_check(launch_gram_packed(G, cplx, d_in, w, w.packed, s), "tensor-core Gram launch"));
     else
       launch_gram_fp32(G, cplx, d_in, w, s);
-    PD_TRY(cuda_check(launch_eig(cplx, n, ep, w, s, ad), "eigensolver launch"));
+    if (p->precision == PD_PRECISION_MIXED && p->method == PD_METHOD_RAW && sub_supported(cplx, n, (int)g->rows)) {
+      // the subspace solver for the patches it certifies, the full solver for the rest
+      PD_TRY(cuda_check(launch_sub(cplx, n, ep, w, s), "subspace eigensolver launch"));
+      EigParams rest = ep;
+      rest.only_unfinished = 1;
+      PD_TRY(cuda_check(launch_eig(cplx, n, rest, w, s, ad), "eigensolver launch"));
+    } else {
+      PD_TRY(cuda_check(launch_eig(cplx, n, ep, w, s, ad), "eigensolver launch"));
+    }
     SynthArgs sa;
     sa.recombination = p->recombination;
     sa.out = d_out_acc;

@@ -777,6 +777,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
   const EigLayout L = eig_layout(CPLX, n, (in_smem & 1) != 0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int p = blockIdx.x;
+  if (ep.only_unfinished && w.n_active[p] >= 0) return;  // solved by k_sub
   T* G = reinterpret_cast<T*>(w.gram + (int64_t)p * w.gram_stride);
   T* A = (in_smem & 1) ? reinterpret_cast<T*>(sm + L.a) : G;
   float* d = reinterpret_cast<float*>(sm + L.d);

@@ -58,11 +58,16 @@ struct EigParams {
   double threshold;
   double mp_median;
   const double* d_threshold;  // raw / NORDIC: read the threshold here when not NULL
+  int only_unfinished;        // 1: solve only the patches with n_active < 0 (left by k_sub)
 };
 constexpr int EIG_MODE_TOP1 = 100;
 cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s,
                        const pd_adaptive* ad = nullptr);
 size_t eig_smem_bytes(bool cplx, int n, bool* in_smem);
+
+// pd_sub.cu: subspace solver of the hard-threshold rule (mixed precision path)
+bool sub_supported(bool cplx, int n, int rows);
+cudaError_t launch_sub(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s);
 
 // pd_synth.cu
 struct SynthArgs {

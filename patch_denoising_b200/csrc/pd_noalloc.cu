@@ -15,8 +15,6 @@
 // rejected with PD_ERR_WORKSPACE.
 #include <cuda_runtime.h>
 
-#include <mutex>
-
 #include "pd_common.cuh"
 
 #define PD_NOALLOC_SCRATCH_BYTES (32u << 20)
@@ -31,9 +29,25 @@ void set_last_error(const char* msg);
 }
 
 namespace {
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_scratch_ptr[kMaxDevices] = {};
+// Device address of the scratch array on the current device. Looked up on every
+// call (a cheap runtime query once the module is loaded), so the address stays
+// right after a device reset or a re-created primary context. The first call
+// on a device loads the library's device code there: make it before any stream
+// capture.
+pd_status scratch_address(void** ptr) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    pd::set_last_error("no usable current CUDA device");
+    return PD_ERR_CUDA;
+  }
+  void* addr = nullptr;
+  if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || addr == nullptr) {
+    pd::set_last_error("cudaGetSymbolAddress of the static scratch array failed");
+    return PD_ERR_CUDA;
+  }
+  *ptr = addr;
+  return PD_OK;
+}
 }  // namespace
 
 extern "C" pd_status pd_denoise_patches_noalloc(const pd_geometry* g, const pd_params* p, const void* d_in,
@@ -51,31 +65,22 @@ extern "C" pd_status pd_denoise_patches_noalloc(const pd_geometry* g, const pd_p
         "use pd_denoise_patches with a caller-allocated workspace");
     return PD_ERR_WORKSPACE;
   }
-  // Device address of the scratch array for the current device, set up once per
-  // device (the first call on a device does this; make that call before any
-  // stream capture).
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-    pd::set_last_error("pd_denoise_patches_noalloc: no usable current CUDA device");
-    return PD_ERR_CUDA;
-  }
   void* ptr = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_ptr[dev]) {
-      void* addr = nullptr;
-      if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || addr == nullptr) {
-        pd::set_last_error("pd_denoise_patches_noalloc: cudaGetSymbolAddress of the static scratch array failed");
-        return PD_ERR_CUDA;
-      }
-      g_scratch_ptr[dev] = addr;
-    }
-    ptr = g_scratch_ptr[dev];
-  }
+  st = scratch_address(&ptr);
+  if (st != PD_OK) return st;
   // pd_denoise_patches clears the device error word at the start of every call
   // and fully writes every scratch buffer it reads; calls whose work overlaps on
   // the GPU (other streams, other host threads) share this array and race.
   return pd_denoise_patches(g, p, d_in, d_noise_std, d_patch_list, n_selected, d_out_acc, d_weight_acc, d_noise_acc,
                             d_noise_ctr, d_rank_map, d_patch_rank, d_patch_noise, ptr, PD_NOALLOC_SCRATCH_BYTES,
                             stream);
+}
+
+// The device error word of the last pd_denoise_patches_noalloc call on this
+// stream (it sits at the start of the static array): pd_workspace_check on it.
+extern "C" pd_status pd_noalloc_check(void* stream) {
+  void* ptr = nullptr;
+  const pd_status st = scratch_address(&ptr);
+  if (st != PD_OK) return st;
+  return pd_workspace_check(ptr, stream);
 }

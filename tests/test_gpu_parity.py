@@ -222,3 +222,15 @@ def test_nordic_monte_carlo_mixed_matches_fp32():
     b = _engine.nordic_max_sval(11**3 * 200, 200, 4, seed=11, device=dev, precision="mixed")
     # same Gaussian draws; bf16 operands perturb the largest singular value by far less than 1e-3
     assert abs(a - b) / a < 1e-3
+
+
+# ------------------------------------------------ subspace solver (mixed, hard threshold)
+@pytest.mark.parametrize("cplx", [False, True])
+def test_raw_mixed_subspace_and_fallback(cplx):
+    """A threshold above the noise keeps few components (the subspace solver
+    certifies them); one inside the noise keeps more than its 16-column block
+    holds, so every patch goes to the full eigensolver. Both match the oracle."""
+    x, _ = lowrank_volume((26, 24, 18, 120), 5, noise=3.0, seed=41, complex_valued=cplx)
+    for thr in (400.0, 20.0):
+        call = dict(method="raw", patch_shape=9, patch_overlap=4, recombination="weighted", threshold_value=thr)
+        compare(call, x, precision="mixed")
