@@ -3,12 +3,13 @@
 // patch finds the eigenpairs of the scaled Gram C that lie above the known
 // threshold, without reducing the whole matrix to tridiagonal form.
 //
-//  1. Block power iteration on P = 16 columns: Y = C Q, then Q = orth(Y) by
-//     Cholesky QR applied twice (CholQR2: the P x P Gram Y^H Y and its Cholesky
-//     factor in FP64, Q = Y R^-1 in FP32). Columns converge to the eigenvectors
-//     above the bulk at the rate lambda_{P+1} / lambda_i per step.
+//  1. Block power iteration on P columns: Y = C Q, then Q = orth(Y) by
+//     Cholesky QR (the P x P Gram Y^H Y, its Cholesky factor R and R^-1 in
+//     FP64, Q = Y R^-1 in FP32), a second pass
+//     before each Rayleigh-Ritz check (CholQR2). Columns converge to the
+//     eigenvectors above the bulk at the rate lambda_{P+1} / lambda_i per step.
 //  2. Rayleigh-Ritz: Z = C Q, H = Q^H Z (P x P Hermitian), cyclic Jacobi
-//     eigensolver of H in FP32 (parallel round-robin ordering), Ritz vectors
+//     eigensolver of H in FP32 (round-robin ordering, one warp), Ritz vectors
 //     V = Q W, C V = Z W and their residuals ||C v_i - theta_i v_i||.
 //  3. The reference rule rank = #{ sqrt(theta_i) > threshold } on the Ritz
 //     values (FP64), accepted only when it is certified: fewer than P Ritz
@@ -21,7 +22,10 @@
 //     Householder solver on it.
 //
 // C stays in shared memory (packed lower, FP32) for every product; the solver
-// applies where that and the P-column blocks fit (sub_supported).
+// applies where that and the P-column blocks fit (sub_supported). A first pass
+// runs with P = 8 columns, which certifies patches that keep up to 7
+// components; the patches it leaves get a pass with P = 16 (up to 15), and any
+// still left get k_eig.
 #include <float.h>
 
 #include "pd_common.cuh"
@@ -32,51 +36,62 @@ namespace pd {
 
 constexpr int SUB_THREADS = 512;
 constexpr int SUB_NW = SUB_THREADS / 32;
-constexpr int SUB_P = 16;        // block columns
 constexpr int SUB_FIRST = 3;     // power steps before the first Rayleigh-Ritz check
 constexpr int SUB_MORE = 2;      // power steps between later checks
 constexpr int SUB_CHECKS = 4;    // checks before the patch goes to k_eig
-constexpr int SUB_SWEEPS = 10;   // Jacobi sweeps at most
+constexpr int SUB_SWEEPS = 8;    // Jacobi sweeps at most
 constexpr float SUB_TOLR = 2e-5f;
 constexpr size_t SUB_SMEM_LIMIT = 227 * 1024 - 1024;
 
 struct SubLayout {
-  size_t a, q, y, g, rinv, h, w, th, perm, res, total;
+  size_t a, q, y, g, part, r, h, w, th, perm, res, total;
+  int slices;  // row slices of the P x P Gram products (partials in `part`)
 };
 
 __host__ __device__ inline size_t sub_al(size_t x) { return (x + 15) & ~size_t(15); }
 
-__host__ __device__ inline SubLayout sub_layout(bool cplx, int n) {
+__host__ __device__ inline SubLayout sub_layout_s(bool cplx, int n, int P, int slices) {
   const size_t es = cplx ? 8 : 4;
+  const size_t PP = (size_t)P * P;
   SubLayout L;
   size_t o = 0;
+  L.slices = slices;
   L.a = o;
   o += sub_al((size_t)pk_size(n) * es);
   L.q = o;
-  o += sub_al((size_t)n * SUB_P * es);
+  o += sub_al((size_t)n * P * es);
   L.y = o;
-  o += sub_al((size_t)n * SUB_P * es);
+  o += sub_al((size_t)n * P * es);
   L.g = o;
-  o += sub_al((size_t)SUB_P * SUB_P * 16);  // FP64 complex Gram (real: imaginary parts stay 0)
-  L.rinv = o;
-  o += sub_al((size_t)SUB_P * SUB_P * es);
+  o += sub_al(PP * 16);  // FP64 complex Gram (real: imaginary parts stay 0)
+  L.part = o;
+  o += slices > 1 ? sub_al(PP * 16 * slices) : 0;
+  L.r = o;
+  o += sub_al(PP * es);  // R^-1 of the Cholesky factor, FP32
   L.h = o;
-  o += sub_al((size_t)SUB_P * SUB_P * es);
+  o += sub_al(PP * es);
   L.w = o;
-  o += sub_al((size_t)SUB_P * SUB_P * es);
+  o += sub_al(PP * es);
   L.th = o;
-  o += sub_al(SUB_P * 4);
+  o += sub_al((size_t)P * 4);
   L.perm = o;
-  o += sub_al(SUB_P * 4);
+  o += sub_al((size_t)P * 4);
   L.res = o;
-  o += sub_al((size_t)SUB_NW * SUB_P * 4);
+  o += sub_al((size_t)P * 4);
   L.total = o;
   return L;
 }
 
-bool sub_supported(bool cplx, int n, int rows) {
-  return n >= 3 * SUB_P && rows > 2 * SUB_P && sub_layout(cplx, n).total <= SUB_SMEM_LIMIT;
+__host__ __device__ inline SubLayout sub_layout(bool cplx, int n, int P) {
+  const SubLayout two = sub_layout_s(cplx, n, P, 2);
+  return two.total <= SUB_SMEM_LIMIT ? two : sub_layout_s(cplx, n, P, 1);
 }
+
+static bool sub_fits(bool cplx, int n, int rows, int P) {
+  return n >= 3 * P && rows > 2 * P && sub_layout(cplx, n, P).total <= SUB_SMEM_LIMIT;
+}
+
+bool sub_supported(bool cplx, int n, int rows) { return sub_fits(cplx, n, rows, 8); }
 
 // ---------------------------------------------------------------------------
 // Small helpers (T = float or cf)
@@ -94,76 +109,143 @@ __device__ __forceinline__ float from_d2<float>(double2 v) { return (float)v.x; 
 template <>
 __device__ __forceinline__ cf from_d2<cf>(double2 v) { return cf{(float)v.x, (float)v.y}; }
 
+// acc[0..NH) += c * Q[k][NH h .. NH h + NH)
+template <bool CPLX, int NH>
+__device__ __forceinline__ void sub_fma(typename Elem<CPLX>::T* acc, typename Elem<CPLX>::T c, const float4* q4) {
+  if constexpr (CPLX) {
+#pragma unroll
+    for (int j = 0; j < NH / 2; ++j) {
+      const float4 v = q4[j];
+      acc[2 * j] = acc[2 * j] + c * cf{v.x, v.y};
+      acc[2 * j + 1] = acc[2 * j + 1] + c * cf{v.z, v.w};
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < NH / 4; ++j) {
+      const float4 v = q4[j];
+      acc[4 * j] += c * v.x;
+      acc[4 * j + 1] += c * v.y;
+      acc[4 * j + 2] += c * v.z;
+      acc[4 * j + 3] += c * v.w;
+    }
+  }
+}
+
 // Y = C Q over the packed lower C (n x n Hermitian), Q and Y row-major n x P.
-// A warp owns 16 rows; lane (r, h) accumulates row r against columns 8h..8h+7.
-// C(row, k) is the stored column-k entry for row >= k, else the conjugate of
-// the entry stored in column row at row k.
-template <bool CPLX>
+// A warp owns 16 rows r0..r0+15; lane (r, h) accumulates row r0 + r against
+// columns (P/2) h .. (P/2) h + P/2 - 1. C(row, k) is the stored column-k entry for row >= k (every
+// k < r0), else the conjugate of the entry stored in column row at row k
+// (every k >= r0 + 16); only the 16 k of the diagonal block take both forms.
+template <bool CPLX, int P>
 __device__ void sub_product(const typename Elem<CPLX>::T* __restrict__ A, int n,
                             const typename Elem<CPLX>::T* __restrict__ Q, typename Elem<CPLX>::T* __restrict__ Y) {
   using T = typename Elem<CPLX>::T;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int r = lane & 15, h = lane >> 4;
   for (int rb = warp; rb * 16 < n; rb += SUB_NW) {
-    const int row = rb * 16 + r;
+    const int r0 = rb * 16, row = r0 + r;
     const bool live = row < n;
-    const int64_t cbr = live ? pk(row, row, n) - row : 0;
-    T acc[8];
+    const int rowc = live ? row : n - 1;  // clamped: loads stay in bounds, results are dropped
+    const int cbr = (int)pk(rowc, rowc, n) - rowc;
+    constexpr int NH = P / 2;
+    T acc[NH];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[j] = zero<T>();
-    int64_t cbk = 0;  // pk(k, k, n) - k
-    for (int k = 0; k < n; ++k) {
-      T c = zero<T>();
-      if (live) c = row >= k ? A[cbk + row] : cj(A[cbr + k]);
-      const float4* q4 = reinterpret_cast<const float4*>(Q + (int64_t)k * SUB_P + h * 8);
-      if constexpr (CPLX) {
+    for (int j = 0; j < NH; ++j) acc[j] = zero<T>();
+    const float4* qb = reinterpret_cast<const float4*>(Q) + h * (NH * sizeof(T) / 16);
+    constexpr int QS = P * sizeof(T) / 16;  // float4 per row of Q
+    int cbk = 0;                                // pk(k, k, n) - k
+    int k = 0;
+    for (; k + 4 <= r0; k += 4) {
+      T c[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const float4 v = q4[j];
-          acc[2 * j] = acc[2 * j] + c * cf{v.x, v.y};
-          acc[2 * j + 1] = acc[2 * j + 1] + c * cf{v.z, v.w};
-        }
-      } else {
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          const float4 v = q4[j];
-          acc[4 * j] += c * v.x;
-          acc[4 * j + 1] += c * v.y;
-          acc[4 * j + 2] += c * v.z;
-          acc[4 * j + 3] += c * v.w;
-        }
+      for (int u = 0; u < 4; ++u) {
+        c[u] = A[cbk + rowc];
+        cbk += n - (k + u) - 1;
       }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) sub_fma<CPLX, NH>(acc, c[u], qb + (k + u) * QS);
+    }
+    for (; k < r0; ++k) {
+      sub_fma<CPLX, NH>(acc, A[cbk + rowc], qb + k * QS);
       cbk += n - k - 1;
     }
+    const int ke = min(r0 + 16, n);
+    for (; k < ke; ++k) {
+      const T c = rowc >= k ? A[cbk + rowc] : cj(A[cbr + k]);
+      sub_fma<CPLX, NH>(acc, c, qb + k * QS);
+      cbk += n - k - 1;
+    }
+    for (; k + 4 <= n; k += 4) {
+      T c[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) c[u] = cj(A[cbr + k + u]);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) sub_fma<CPLX, NH>(acc, c[u], qb + (k + u) * QS);
+    }
+    for (; k < n; ++k) sub_fma<CPLX, NH>(acc, cj(A[cbr + k]), qb + k * QS);
     if (live) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) Y[(int64_t)row * SUB_P + h * 8 + j] = acc[j];
+      for (int j = 0; j < NH; ++j) Y[row * P + h * NH + j] = acc[j];
     }
   }
 }
 
-// Q = orth(Y) by one Cholesky-QR pass: G = Y^H Y (FP64), G = R^H R (warp 0,
-// FP64), Q = Y R^-1. Returns false (on every thread) if G is not numerically
-// positive definite. Ends with a block barrier.
-template <bool CPLX>
-__device__ bool sub_cholqr(int n, const typename Elem<CPLX>::T* __restrict__ Y, typename Elem<CPLX>::T* __restrict__ Q,
-                           double2* G, typename Elem<CPLX>::T* Rinv, int* s_ok) {
-  using T = typename Elem<CPLX>::T;
-  const int tid = threadIdx.x, lane = tid & 31;
-  constexpr int P = SUB_P;
-  // Gram: a thread per upper entry (a <= b)
-  for (int t = tid; t < P * P; t += SUB_THREADS) {
-    const int a = t / P, b = t % P;
+// G_ab = sum_r conj(X_ra) Y_rb (FP64) for a <= b, over L.slices row slices
+// (partials in `part`, then summed). Ends with a block barrier.
+template <bool CPLX, int P>
+__device__ void sub_gram(int n, const typename Elem<CPLX>::T* __restrict__ X,
+                         const typename Elem<CPLX>::T* __restrict__ Yv, double2* G, double2* part, int slices) {
+  constexpr int PP = P * P;
+  const int tid = threadIdx.x;
+  for (int t = tid; t < PP * slices; t += SUB_THREADS) {
+    const int u = t % PP, sl = t / PP;
+    const int a = u / P, b = u % P;
     if (a > b) continue;
-    double sr = 0.0, si = 0.0;
-    for (int r = 0; r < n; ++r) {
-      const double2 v = d2conjmul(Y[(int64_t)r * P + a], Y[(int64_t)r * P + b]);
-      sr += v.x;
-      si += v.y;
+    const int rlo = sl * n / slices, rhi = (sl + 1) * n / slices;
+    double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
+    int r = rlo;
+    for (; r + 2 <= rhi; r += 2) {
+      const double2 v0 = d2conjmul(X[r * P + a], Yv[r * P + b]);
+      const double2 v1 = d2conjmul(X[(r + 1) * P + a], Yv[(r + 1) * P + b]);
+      sr0 += v0.x;
+      si0 += v0.y;
+      sr1 += v1.x;
+      si1 += v1.y;
     }
-    G[a * P + b] = make_double2(sr, si);
+    if (r < rhi) {
+      const double2 v0 = d2conjmul(X[r * P + a], Yv[r * P + b]);
+      sr0 += v0.x;
+      si0 += v0.y;
+    }
+    const double2 v = make_double2(sr0 + sr1, si0 + si1);
+    if (slices == 1) G[u] = v;
+    else part[t] = v;
   }
   __syncthreads();
+  if (slices > 1) {
+    for (int u = tid; u < PP; u += SUB_THREADS) {
+      if (u / P > u % P) continue;
+      double2 v = part[u];
+      for (int sl = 1; sl < slices; ++sl) {
+        v.x += part[sl * PP + u].x;
+        v.y += part[sl * PP + u].y;
+      }
+      G[u] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// Q = orth(Y) by one Cholesky-QR pass: G = Y^H Y (FP64), G = R^H R and R^-1
+// (warp 0, FP64; R^-1 stored in FP32 in R), Q = Y R^-1. Returns false (on
+// every thread) if G is not numerically positive definite. Ends with a block
+// barrier.
+template <bool CPLX, int P>
+__device__ bool sub_cholqr(int n, const typename Elem<CPLX>::T* __restrict__ Y, typename Elem<CPLX>::T* __restrict__ Q,
+                           double2* G, double2* part, int slices, typename Elem<CPLX>::T* R, int* s_ok) {
+  using T = typename Elem<CPLX>::T;
+  const int tid = threadIdx.x, lane = tid & 31;
+  sub_gram<CPLX, P>(n, Y, Y, G, part, slices);
   if (tid < 32) {
     // right-looking Cholesky on the upper triangle: lane j owns column j
     const double g00 = G[0].x;
@@ -177,8 +259,8 @@ __device__ bool sub_cholqr(int n, const typename Elem<CPLX>::T* __restrict__ Y, 
         const double2 gk = G[k * P + lane];
         G[k * P + lane] = make_double2(gk.x / rkk, gk.y / rkk);
       }
-      __syncwarp();
       if (lane == k) G[k * P + k] = make_double2(rkk, 0.0);
+      __syncwarp();
       if (lane > k && lane < P) {
         const double2 rkj = G[k * P + lane];
         for (int i = k + 1; i <= lane; ++i) {
@@ -191,83 +273,84 @@ __device__ bool sub_cholqr(int n, const typename Elem<CPLX>::T* __restrict__ Y, 
       }
       __syncwarp();
     }
-    // R^-1 (upper): lane j solves R x = e_j by back substitution
+    // R^-1 (upper): lane j back-substitutes column j in FP64; x_i (i < j) is
+    // kept in the unused lower triangle of G at (j, i), x_j = 1 / R_jj
     if (lane < P) {
       const int j = lane;
-      double2 x[P];
-#pragma unroll
-      for (int i = 0; i < P; ++i) x[i] = make_double2(0.0, 0.0);
-      for (int i = j; i >= 0; --i) {
-        double2 acc = make_double2(i == j ? 1.0 : 0.0, 0.0);
+      const double xj = 1.0 / G[j * P + j].x;
+      for (int i = j - 1; i >= 0; --i) {
+        double ar = 0.0, ai = 0.0;
         for (int k = i + 1; k <= j; ++k) {
           const double2 rik = G[i * P + k];
-          acc.x -= rik.x * x[k].x - rik.y * x[k].y;
-          acc.y -= rik.x * x[k].y + rik.y * x[k].x;
+          const double2 xk = k == j ? make_double2(xj, 0.0) : G[j * P + k];
+          ar += rik.x * xk.x - rik.y * xk.y;
+          ai += rik.x * xk.y + rik.y * xk.x;
         }
         const double rii = G[i * P + i].x;
-        x[i] = make_double2(acc.x / rii, acc.y / rii);
+        G[j * P + i] = make_double2(-ar / rii, -ai / rii);
       }
-#pragma unroll
-      for (int i = 0; i < P; ++i) Rinv[i * P + j] = from_d2<T>(x[i]);
+    }
+    __syncwarp();
+    for (int u = lane; u < P * P; u += 32) {
+      const int a = u / P, c = u % P;
+      R[u] = a < c ? from_d2<T>(G[c * P + a]) : (a == c ? from_d2<T>(make_double2(1.0 / G[c * P + c].x, 0.0))
+                                                          : zero<T>());
     }
     if (lane == 0) *s_ok = ok ? 1 : 0;
   }
   __syncthreads();
   const bool ok = *s_ok != 0;
-  // Q = Y R^-1, a thread per (row, column)
+  // Q = Y R^-1, a thread per entry
   for (int t = tid; t < n * P; t += SUB_THREADS) {
     const int r = t / P, c = t % P;
     T acc = zero<T>();
-    for (int a = 0; a <= c; ++a) acc = acc + mul(Y[(int64_t)r * P + a], Rinv[a * P + c]);
-    Q[(int64_t)r * P + c] = acc;
+    for (int a = 0; a <= c; ++a) acc = acc + mul(Y[r * P + a], R[a * P + c]);
+    Q[t] = acc;
   }
   __syncthreads();
   return ok;
 }
 
-// Eigenpairs of the P x P Hermitian H (full storage, overwritten): cyclic
-// Jacobi with the round-robin ordering, P/2 disjoint rotations per round, run
-// by warps 0-1 with a named barrier (the other warps return at once). W
-// receives the eigenvectors (columns), diag(H) the eigenvalues. For the pair
+// Eigenpairs of the P x P Hermitian H (full storage, overwritten) by warp 0:
+// cyclic Jacobi with the round-robin ordering, P/2 disjoint rotations per round.
+// W receives the eigenvectors (columns), diag(H) the eigenvalues. For the pair
 // (p, q) with H_pq = |b| e^{i phi}, J = diag(1, e^{-i phi}) R, R the real
 // rotation that diagonalises [[H_pp, |b|], [|b|, H_qq]] (t the smaller root of
 // t^2 + 2 tau t - 1 = 0, tau = (H_qq - H_pp) / (2 |b|); Golub & Van Loan 8.5.2).
-template <bool CPLX>
+// The other warps return at once.
+template <bool CPLX, int P>
 __device__ void sub_jacobi(typename Elem<CPLX>::T* H, typename Elem<CPLX>::T* W) {
   using T = typename Elem<CPLX>::T;
-  constexpr int P = SUB_P, NP = SUB_P / 2;
-  const int tid = threadIdx.x;
+  constexpr int NP = P / 2;
+  const int lane = threadIdx.x;
   __shared__ float s_c[NP], s_s[NP], s_er[NP], s_ei[NP];
   __shared__ int s_p[NP], s_q[NP];
-  __shared__ int s_stop;
-  if (tid >= 64) return;
-  auto bar = [] { asm volatile("bar.sync 1, 64;" ::: "memory"); };
-  for (int t = tid; t < P * P; t += 64) {
+  if (threadIdx.x >= 32) return;
+  for (int t = lane; t < P * P; t += 32) {
     if constexpr (CPLX) W[t] = cf{(t / P) == (t % P) ? 1.f : 0.f, 0.f};
     else W[t] = (t / P) == (t % P) ? 1.f : 0.f;
   }
-  bar();
+  __syncwarp();
   for (int sweep = 0; sweep < SUB_SWEEPS; ++sweep) {
     // stop once every off-diagonal entry is negligible against the diagonal
-    if (tid == 0) {
-      float off = 0.f, dg = 0.f;
-      for (int i = 0; i < P; ++i) {
-        dg = fmaxf(dg, fabsf(re(H[i * P + i])));
-        for (int j = i + 1; j < P; ++j) off = fmaxf(off, sqrtf(abs2(H[i * P + j])));
-      }
-      s_stop = (off <= 1e-7f * dg) ? 1 : 0;
+    float off = 0.f, dg = 0.f;
+    for (int t = lane; t < P * P; t += 32) {
+      const int i = t / P, j = t % P;
+      if (i == j) dg = fmaxf(dg, fabsf(re(H[t])));
+      else if (i < j) off = fmaxf(off, abs2(H[t]));
     }
-    bar();
-    if (s_stop) break;
+    off = warp_max(off);
+    dg = warp_max(dg);
+    if (off <= 1e-12f * dg * dg) break;
     for (int round = 0; round < P - 1; ++round) {
-      if (tid < NP) {
+      if (lane < NP) {
         int p, q;
-        if (tid == 0) {
+        if (lane == 0) {
           p = round;
           q = P - 1;
         } else {
-          p = (round + tid) % (P - 1);
-          q = (round - tid + (P - 1)) % (P - 1);
+          p = (round + lane) % (P - 1);
+          q = (round - lane + (P - 1)) % (P - 1);
         }
         if (p > q) {
           const int t = p;
@@ -290,16 +373,17 @@ __device__ void sub_jacobi(typename Elem<CPLX>::T* H, typename Elem<CPLX>::T* W)
             er = b / ab;  // sign of b
           }
         }
-        s_c[tid] = c;
-        s_s[tid] = s;
-        s_er[tid] = er;
-        s_ei[tid] = ei;
-        s_p[tid] = p;
-        s_q[tid] = q;
+        s_c[lane] = c;
+        s_s[lane] = s;
+        s_er[lane] = er;
+        s_ei[lane] = ei;
+        s_p[lane] = p;
+        s_q[lane] = q;
       }
-      bar();
+      __syncwarp();
       // rows: [H_p.; H_q.] <- J^H [H_p.; H_q.], J = [[c, s], [-s e^{-i phi}, c e^{-i phi}]]
-      for (int t = tid; t < NP * P; t += 64) {
+#pragma unroll
+      for (int t = lane; t < NP * P; t += 32) {
         const int k = t / P, j = t % P;
         const int p = s_p[k], q = s_q[k];
         const float c = s_c[k], s = s_s[k];
@@ -314,9 +398,10 @@ __device__ void sub_jacobi(typename Elem<CPLX>::T* H, typename Elem<CPLX>::T* W)
           H[q * P + j] = s * hp + c * eq;
         }
       }
-      bar();
+      __syncwarp();
       // columns: [H_.p, H_.q] <- [H_.p, H_.q] J; the same for W
-      for (int t = tid; t < 2 * NP * P; t += 64) {
+#pragma unroll
+      for (int t = lane; t < 2 * NP * P; t += 32) {
         const int which = t / (NP * P), u = t % (NP * P);
         const int k = u / P, i = u % P;
         T* X = which ? W : H;
@@ -333,7 +418,7 @@ __device__ void sub_jacobi(typename Elem<CPLX>::T* H, typename Elem<CPLX>::T* W)
           X[i * P + q] = s * xp + c * xe;
         }
       }
-      bar();
+      __syncwarp();
     }
   }
 }
@@ -341,32 +426,39 @@ __device__ void sub_jacobi(typename Elem<CPLX>::T* H, typename Elem<CPLX>::T* W)
 // ---------------------------------------------------------------------------
 // The kernel: one CTA per patch; n_active = -1 hands the patch to k_eig.
 // ---------------------------------------------------------------------------
-template <bool CPLX>
+template <bool CPLX, int P>
 __global__ void __launch_bounds__(SUB_THREADS, 1) k_sub(int n, EigParams ep, PatchWork w) {
   using T = typename Elem<CPLX>::T;
-  constexpr int P = SUB_P;
   extern __shared__ __align__(16) unsigned char sm[];
-  const SubLayout L = sub_layout(CPLX, n);
+  const SubLayout L = sub_layout(CPLX, n, P);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int p = blockIdx.x;
+  if (ep.only_unfinished && w.n_active[p] >= 0) return;  // certified by an earlier pass
   T* A = reinterpret_cast<T*>(sm + L.a);
   T* q = reinterpret_cast<T*>(sm + L.q);
   T* y = reinterpret_cast<T*>(sm + L.y);
   double2* G = reinterpret_cast<double2*>(sm + L.g);
-  T* Rinv = reinterpret_cast<T*>(sm + L.rinv);
+  double2* part = reinterpret_cast<double2*>(sm + L.part);
+  T* R = reinterpret_cast<T*>(sm + L.r);
   T* H = reinterpret_cast<T*>(sm + L.h);
   T* W = reinterpret_cast<T*>(sm + L.w);
   float* th = reinterpret_cast<float*>(sm + L.th);
   int* perm = reinterpret_cast<int*>(sm + L.perm);
-  float* rpart = reinterpret_cast<float*>(sm + L.res);
+  float* res2 = reinterpret_cast<float*>(sm + L.res);
+  const int S = L.slices;
   __shared__ int s_ok, s_done;
   __shared__ double s_md;
   __shared__ float s_red[SUB_NW];
+  auto swap_qy = [&] {
+    T* t_ = q;
+    q = y;
+    y = t_;
+  };
 
   // stage and scale the Gram (by 1 / max diagonal, as k_eig)
   const T* Gg = reinterpret_cast<const T*>(w.gram + (int64_t)p * w.gram_stride);
-  const int64_t np = pk_size(n);
-  for (int64_t i = tid; i < np; i += SUB_THREADS) A[i] = Gg[i];
+  const int np = (int)pk_size(n);
+  for (int i = tid; i < np; i += SUB_THREADS) A[i] = Gg[i];
   __syncthreads();
   float md = 0.f;
   for (int i = tid; i < n; i += SUB_THREADS) md = fmaxf(md, re(A[pk(i, i, n)]));
@@ -376,7 +468,7 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_sub(int n, EigParams ep, Pat
   md = warp_max(lane < SUB_NW ? s_red[lane] : 0.f);
   const float sc = md > 0.f ? 1.f / md : 1.f;
   if (tid == 0) s_md = md > 0.f ? (double)md : 1.0;
-  for (int64_t i = tid; i < np; i += SUB_THREADS) A[i] = A[i] * sc;
+  for (int i = tid; i < np; i += SUB_THREADS) A[i] = A[i] * sc;
   // pseudo-random start block (a fixed hash of the row and column)
   for (int t = tid; t < n * P; t += SUB_THREADS) {
     uint32_t hsh = (uint32_t)(t + 17) * 2654435761u;
@@ -385,50 +477,40 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_sub(int n, EigParams ep, Pat
     hsh ^= hsh >> 15;
     const float u = (float)(hsh & 0xffff) * (1.f / 65536.f) - 0.5f;
     const float v = (float)(hsh >> 16) * (1.f / 65536.f) - 0.5f;
-    if constexpr (CPLX) y[t] = cf{u, v};
-    else y[t] = u;
+    if constexpr (CPLX) q[t] = cf{u, v};
+    else q[t] = u;
   }
   __syncthreads();
-  bool ok = sub_cholqr<CPLX>(n, y, q, G, Rinv, &s_ok);
-  ok = ok && sub_cholqr<CPLX>(n, q, y, G, Rinv, &s_ok);
-  {
-    T* t_ = q;
-    q = y;
-    y = t_;
-  }
+  bool ok = true;
   const double md64 = s_md;
   const double thr = ep.d_threshold ? *ep.d_threshold : ep.threshold;
   const double thr2s = thr * thr / md64;  // the threshold on scaled eigenvalues
   int steps = SUB_FIRST;
   for (int check = 0; ok && check < SUB_CHECKS; ++check) {
+    // power steps: one Cholesky-QR each, a second one before Rayleigh-Ritz
     for (int it = 0; ok && it < steps; ++it) {
-      sub_product<CPLX>(A, n, q, y);
+      sub_product<CPLX, P>(A, n, q, y);
       __syncthreads();
-      ok = sub_cholqr<CPLX>(n, y, q, G, Rinv, &s_ok);
-      ok = ok && sub_cholqr<CPLX>(n, q, y, G, Rinv, &s_ok);
-      T* t_ = q;
-      q = y;
-      y = t_;
+      ok = sub_cholqr<CPLX, P>(n, y, q, G, part, S, R, &s_ok);
     }
+    ok = ok && sub_cholqr<CPLX, P>(n, q, y, G, part, S, R, &s_ok);
     if (!ok) break;
+    swap_qy();
     // Rayleigh-Ritz: Z = C Q (into y), H = Q^H Z
-    sub_product<CPLX>(A, n, q, y);
+    sub_product<CPLX, P>(A, n, q, y);
     __syncthreads();
-    for (int t = tid; t < P * P; t += SUB_THREADS) {
-      const int a = t / P, b = t % P;
+    sub_gram<CPLX, P>(n, q, y, G, part, S);
+    for (int u = tid; u < P * P; u += SUB_THREADS) {
+      const int a = u / P, b = u % P;
       if (a > b) continue;
-      double sr = 0.0, si = 0.0;
-      for (int r = 0; r < n; ++r) {
-        const double2 v = d2conjmul(q[(int64_t)r * P + a], y[(int64_t)r * P + b]);
-        sr += v.x;
-        si += v.y;
-      }
-      if (a == b) si = 0.0;
-      H[a * P + b] = from_d2<T>(make_double2(sr, si));
-      H[b * P + a] = from_d2<T>(make_double2(sr, -si));
+      double2 v = G[u];
+      if (a == b) v.y = 0.0;
+      H[a * P + b] = from_d2<T>(v);
+      H[b * P + a] = from_d2<T>(make_double2(v.x, -v.y));
     }
+    if (tid < P) res2[tid] = 0.f;
     __syncthreads();
-    sub_jacobi<CPLX>(H, W);
+    sub_jacobi<CPLX, P>(H, W);
     __syncthreads();
     // descending order of the Ritz values
     if (tid < P) {
@@ -442,57 +524,42 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_sub(int n, EigParams ep, Pat
       th[rk] = v;
     }
     __syncthreads();
-    // V = Q W and C V = Z W in sorted order, in place (a thread per row), with
-    // per-warp partial sums of the squared residuals
-    float r2[P];
-#pragma unroll
-    for (int i = 0; i < P; ++i) r2[i] = 0.f;
-    for (int r = tid; r < n; r += SUB_THREADS) {
-      T qr[P], vr[P];
-#pragma unroll
-      for (int a = 0; a < P; ++a) qr[a] = q[(int64_t)r * P + a];
-#pragma unroll
-      for (int i = 0; i < P; ++i) {
+    // V = Q W and C V = Z W in sorted order, in place: a warp owns 32 / P rows
+    // (a lane per entry), reads them, then overwrites them; the squared residuals
+    // |(C V)_ri - theta_i V_ri|^2 are summed per column
+    for (int base = warp * 32; base < n * P; base += SUB_THREADS) {
+      const int t = base + lane;
+      const bool act = t < n * P;
+      const int r = act ? t / P : 0, i = t % P;
+      T v = zero<T>(), z = zero<T>();
+      if (act) {
         const int c = perm[i];
-        T acc = zero<T>();
 #pragma unroll
-        for (int a = 0; a < P; ++a) acc = acc + mul(qr[a], W[a * P + c]);
-        vr[i] = acc;
+        for (int a = 0; a < P; ++a) {
+          const T wac = W[a * P + c];
+          v = v + mul(q[r * P + a], wac);
+          z = z + mul(y[r * P + a], wac);
+        }
+      }
+      __syncwarp();
+      float e2 = 0.f;
+      if (act) {
+        q[r * P + i] = v;
+        y[r * P + i] = z;
+        e2 = abs2(z - v * th[i]);
       }
 #pragma unroll
-      for (int a = 0; a < P; ++a) {
-        q[(int64_t)r * P + a] = vr[a];
-        qr[a] = y[(int64_t)r * P + a];
-      }
-#pragma unroll
-      for (int i = 0; i < P; ++i) {
-        const int c = perm[i];
-        T acc = zero<T>();
-#pragma unroll
-        for (int a = 0; a < P; ++a) acc = acc + mul(qr[a], W[a * P + c]);
-        y[(int64_t)r * P + i] = acc;
-        r2[i] += abs2(acc - vr[i] * th[i]);
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < P; ++i) {
-      const float s = warp_sum(r2[i]);
-      if (lane == 0) rpart[warp * P + i] = s;
+      for (int o = 16; o >= P; o >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, o);
+      if (lane < P) atomicAdd(&res2[lane], e2);
     }
     __syncthreads();
     if (tid == 0) {
-      float res[P];
-      for (int i = 0; i < P; ++i) {
-        float s = 0.f;
-        for (int k = 0; k < SUB_NW; ++k) s += rpart[k * P + i];
-        res[i] = sqrtf(s);
-      }
       // the reference rule on the Ritz values: s_i = sqrt(theta_i) > threshold
       int cnt = 0;
       while (cnt < P && sqrt(fmax((double)th[cnt], 0.0) * md64) > thr) ++cnt;
       bool cert = cnt < P && (double)th[P - 1] < 0.25 * thr2s;
-      for (int i = 0; cert && i < cnt; ++i) cert = res[i] <= SUB_TOLR * th[i];
-      if (cert) cert = (double)th[cnt] + (double)res[cnt] < thr2s;
+      for (int i = 0; cert && i < cnt; ++i) cert = sqrtf(res2[i]) <= SUB_TOLR * th[i];
+      if (cert) cert = (double)th[cnt] + sqrt((double)res2[cnt]) < thr2s;
       s_done = cert ? 1 + cnt : 0;
       if (cert) {
         w.rank[p] = cnt;
@@ -507,7 +574,7 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_sub(int n, EigParams ep, Pat
       float* vbase = w.vec + (int64_t)p * w.vec_stride;
       for (int t = tid; t < act * n; t += SUB_THREADS) {
         const int a = t / n, r = t % n;
-        const T v = q[(int64_t)r * P + a];
+        const T v = q[r * P + a];
         if constexpr (CPLX) reinterpret_cast<cf*>(vbase + (int64_t)a * 2 * n)[r] = v;
         else vbase[(int64_t)a * 2 * n + r] = v;
       }
@@ -515,23 +582,32 @@ __global__ void __launch_bounds__(SUB_THREADS, 1) k_sub(int n, EigParams ep, Pat
       return;
     }
     // the next power step starts from C V (in y)
-    ok = sub_cholqr<CPLX>(n, y, q, G, Rinv, &s_ok);
-    ok = ok && sub_cholqr<CPLX>(n, q, y, G, Rinv, &s_ok);
-    T* t_ = q;
-    q = y;
-    y = t_;
+    ok = sub_cholqr<CPLX, P>(n, y, q, G, part, S, R, &s_ok);
     steps = SUB_MORE - 1;
   }
   if (tid == 0) w.n_active[p] = -1;  // not certified: the full solver takes it
 }
 
-cudaError_t launch_sub(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
-  const size_t smem = sub_layout(cplx, n).total;
-  auto kern = cplx ? k_sub<true> : k_sub<false>;
-  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+template <bool CPLX, int P>
+static cudaError_t sub_pass(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
+  const size_t smem = sub_layout(CPLX, n, P).total;
+  cudaError_t err = cudaFuncSetAttribute(k_sub<CPLX, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
-  PD_TIMED("eig_sub", s, kern<<<w.count, SUB_THREADS, smem, s>>>(n, ep, w));
+  PD_TIMED(P == 8 ? "eig_sub8" : "eig_sub16", s, k_sub<CPLX, P><<<w.count, SUB_THREADS, smem, s>>>(n, ep, w));
   return cudaGetLastError();
+}
+
+// P = 8 on every patch, then P = 16 on the patches it did not certify (when
+// that block fits); the caller's k_eig pass takes what is left.
+cudaError_t launch_sub(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s) {
+  const int rows = ep.rows;
+  EigParams e8 = ep;
+  e8.only_unfinished = 0;
+  cudaError_t err = cplx ? sub_pass<true, 8>(n, e8, w, s) : sub_pass<false, 8>(n, e8, w, s);
+  if (err != cudaSuccess || !sub_fits(cplx, n, rows, 16)) return err;
+  EigParams e16 = ep;
+  e16.only_unfinished = 1;
+  return cplx ? sub_pass<true, 16>(n, e16, w, s) : sub_pass<false, 16>(n, e16, w, s);
 }
 
 }  // namespace pd

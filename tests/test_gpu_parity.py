@@ -234,3 +234,13 @@ def test_raw_mixed_subspace_and_fallback(cplx):
     for thr in (400.0, 20.0):
         call = dict(method="raw", patch_shape=9, patch_overlap=4, recombination="weighted", threshold_value=thr)
         compare(call, x, precision="mixed")
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_raw_mixed_ten_components(cplx):
+    """About ten components above the threshold in every patch: more than the
+    8-column pass can certify, so the 16-column pass (or the full solver)
+    decides them."""
+    x, _ = lowrank_volume((16, 16, 12, 120), 10, noise=3.0, seed=43, complex_valued=cplx)
+    call = dict(method="raw", patch_shape=9, patch_overlap=5, recombination="weighted", threshold_value=250.0)
+    compare(call, x, precision="mixed")
