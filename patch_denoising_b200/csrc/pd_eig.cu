@@ -549,6 +549,10 @@ __device__ double ad_cost(const AdSpec& c, double lt, double gamma) {
   double dv = 0.0, sd = 0.0, rss = 0.0;
   for (int k = lane; k < c.nv; k += 32) {
     const double s = c.s[k];
+    // a zero singular value (a rank-deficient patch, M <= T) adds nothing: in
+    // the limit s -> 0 its d, indicator and d / s terms all vanish, as they do
+    // for the tiny value the reference's SVD returns there
+    if (!(s > 0.0)) continue;
     const double r = exp(gamma * (lt - c.ls[k]));  // (tau / s)^gamma
     const double dh = s * np_max0(1.0 - r);
     dv += (1.0 + (gamma - 1.0) * r) * (s >= tau ? 1.0 : 0.0) + fabs(c.M - c.T) * dh / s;
@@ -691,9 +695,16 @@ __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adap
   for (int k = tid; k < nv; k += EIG_THREADS) {
     const double a2 = sv[k] * sv[k];
     double acc = 0.0;
-    for (int q = 0; q < nv; ++q)
-      if (q != k) acc += 1.0 / (a2 - sv[q] * sv[q]);
+    if (a2 > 0.0)  // zero singular values are skipped by the cost (their si is unused)
+      for (int q = 0; q < nv; ++q)
+        if (q != k) acc += 1.0 / (a2 - sv[q] * sv[q]);
     si[k] = acc;
+  }
+  __shared__ int s_npos;  // positive singular values (descending, so a prefix)
+  if (tid == 0) {
+    int np_ = 0;
+    while (np_ < nv && sv[np_] > 0.0) ++np_;
+    s_npos = np_;
   }
   __syncthreads();
   __shared__ double s_cost[PD_ADAPTIVE_MAX_GAMMA], s_x[PD_ADAPTIVE_MAX_GAMMA];
@@ -718,9 +729,13 @@ __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adap
     // candidate. log tau stays within 10 of the log spectrum: far below the
     // smallest singular value every d equals s to rounding and the GSURE cost
     // is 0/0 (rss and 1 - div/(M T) both vanish with gamma = 1).
-    const double xlo = lsv[nv - 1] - 10.0, xhi = lsv[0] + 10.0;
+    const int npos = s_npos > 0 ? s_npos : 1;
+    const double xlo = lsv[npos - 1] - 10.0, xhi = lsv[0] + 10.0;
     double x0 = ad.tau0;
-    if (!ad.has_tau0) x0 = log((nv & 1) ? sv[nv / 2] : 0.5 * (sv[nv / 2 - 1] + sv[nv / 2]));
+    if (!ad.has_tau0) {
+      const double med = (nv & 1) ? sv[nv / 2] : 0.5 * (sv[nv / 2 - 1] + sv[nv / 2]);
+      x0 = med > 0.0 ? log(med) : xlo;  // a median of zeros: start at the smallest positive value
+    }
     for (int q = warp; q < ad.n_gamma; q += EIG_NW) {
       const double gq = ad.gamma[q];
       const double x = ad_minimize([&](double xx) { return ad_cost(c, xx, gq); }, x0, xlo, xhi);
@@ -751,7 +766,7 @@ __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adap
     for (int k = 0; k < nv; ++k) {
       const double dh = sv[k] * np_max0(1.0 - exp(gq * (lt - lsv[k])));
       if (dh != 0.0) maxidx = k + 1;  // NaN counts as nonzero, as in numpy
-      acoef[k] = (float)(dh / sv[k]);
+      acoef[k] = sv[k] > 0.0 ? (float)(dh / sv[k]) : 0.f;
     }
     for (int k = 0; k < maxidx; ++k) {
       aidx[k] = n - 1 - k;

@@ -75,6 +75,10 @@ class PatchedArray:
         return getattr(self._arr, name)
 
 
+# the methods the CUDA patch loop implements (the per-patch hooks of space_time/lowrank.py)
+_SUPPORTED_METHODS = ("mp-pca", "hybrid-pca", "raw", "nordic", "optimal", "adaptive")
+
+
 def _is_float_scalar(x):
     return isinstance(x, (float, np.floating))
 
@@ -107,6 +111,14 @@ class BaseSpaceTimeDenoiser(abc.ABC):
         self.recombination = recombination
         self.precision = precision
         self.input_denoising_kwargs = dict()
+        overridden = type(self)._patch_processing is not BaseSpaceTimeDenoiser._patch_processing
+        if overridden or self._method not in _SUPPORTED_METHODS:
+            raise NotImplementedError(
+                f"{type(self).__name__}: a custom per-patch _patch_processing is not supported; the patch loop "
+                f"runs on the GPU for the built-in methods only ({', '.join(_SUPPORTED_METHODS)}). Subclass "
+                "MPPCADenoiser, HybridPCADenoiser, RawSVDDenoiser, NordicDenoiser, OptimalSVDDenoiser or "
+                "AdaptiveDenoiser instead."
+            )
 
     def denoise(self, input_data, mask=None, mask_threshold=50, progbar=None):
         """Denoise ``input_data`` (last axis = time) according to ``mask``.

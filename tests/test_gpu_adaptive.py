@@ -53,7 +53,24 @@ def _oracle(x, call, qlevel, override=None):
 @pytest.mark.parametrize("name", adaptive_golden_names())
 def test_adaptive_matches_the_oracle(name, precision):
     arrays, call = load_adaptive_golden(name)
-    x = arrays["input"]
+    _check(arrays["input"], call, precision, name)
+
+
+@pytest.mark.parametrize("method,gamma0", [("sure", [1.0, 2.0, 3.0]), ("gsure", [1.0, 2.0]), ("qut", None),
+                                           ("qut", 2.0)])
+def test_adaptive_rank_deficient_patches(method, gamma0):
+    """Patches with fewer voxels than frames (M = 27 < T = 40): the centred
+    Casorati matrix has a zero singular value, whose cost terms vanish (the
+    reference's SVD returns a tiny one there), so the cost stays finite."""
+    from patch_denoising_b200.synthetic import lowrank_volume
+
+    x, _ = lowrank_volume((12, 11, 9, 40), 3, amplitude=30.0, noise=2.0, seed=77)
+    call = dict(method="adaptive", patch_shape=3, patch_overlap=1, recombination="weighted",
+                adaptive_method=method, noise_std=2.0, nbsim=200, gamma0=gamma0, tau0=None)
+    _check(x, call, "fp32", f"rank-deficient {method}")
+
+
+def _check(x, call, precision, name):
     np.random.seed(11)
     (out, weights, _, rank_map), den = _ours(x, call, precision)
     qlevel = den.qut_level_

@@ -112,6 +112,27 @@ def test_constructor_errors():
         OptimalSVDDenoiser(5, 2, loss="l1")
 
 
+def test_custom_patch_processing_is_rejected_at_construction():
+    """The reference's extension point is a per-patch ``_patch_processing``
+    (base.py:352-357); the CUDA loop cannot call Python per patch, so a subclass
+    that overrides it (or names no built-in method) fails at once with a message
+    that lists the supported methods."""
+    from patch_denoising_b200.space_time.base import BaseSpaceTimeDenoiser
+
+    class Custom(MPPCADenoiser):
+        def _patch_processing(self, patch, patch_idx=None, **kwargs):
+            return patch, 0, 0.0
+
+    class Bare(BaseSpaceTimeDenoiser):
+        def _patch_processing(self, patch, patch_idx=None, **kwargs):
+            return patch, 0, 0.0
+
+    for make in (lambda: Custom(5, 2, 1.0), lambda: Bare(5, 2)):
+        with pytest.raises(NotImplementedError, match="mp-pca, hybrid-pca, raw, nordic, optimal, adaptive"):
+            make()
+    MPPCADenoiser(5, 2, 1.0)  # the built-in classes still construct
+
+
 def test_nordic_noise_std_type_error_before_device_use():
     # space_time/lowrank.py:234-240: a non-float, non-array noise level is a ValueError
     x = np.zeros((10, 10, 10, 20), np.float32)
