@@ -9,8 +9,9 @@ step includes the NORDIC Monte-Carlo level (10 Gaussian draws of 266200 x 200).
 Printed JSON keys: ``value`` = voxel-frames/s with the input resident in HBM;
 ``e2e`` = the same call through the public API on host (NumPy) buffers, copies
 included; ``roofline`` for the dominant kernel from CUDA-event timings taken
-inside the timed region; ``cpu_baseline`` = the CPU oracle (the reference's
-algorithm on NumPy/SciPy LAPACK) timed on a bounded sample of the same workload.
+inside the timed region; ``cpu_baseline`` = one whole call of the CPU oracle
+(the reference's algorithm on NumPy/SciPy LAPACK) on the same volume. The
+reference arm (``--impl reference``) times steps of exactly 1/5 of that call.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision fp32|mixed]
@@ -105,28 +106,27 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- CPU arm
-def cpu_reference_sample(x, mc_draws=1, n_patches=60):
-    """Time the oracle (the reference algorithm on NumPy/SciPy) on a bounded sample.
+SAMPLE_FRACTION = 5  # the reference arm's step: exactly 1/5 of one call
 
-    Sample: ``mc_draws`` of the 10 Monte-Carlo SVDs (266200 x 200) and the first
-    ``n_patches`` of the 405 patches (centred complex SVD, hard threshold,
-    synthesis, weighted accumulation). Both are scaled to the full call.
-    Returns (seconds for the full call, description).
-    """
-    import oracle
+
+def cpu_sample_step(x):
+    """One reference-arm step: exactly 1/SAMPLE_FRACTION of a full NORDIC call on
+    the CPU oracle (the reference's algorithm on NumPy/SciPy LAPACK): 2 of the 10
+    Monte-Carlo SVDs (266200 x 200) and 81 of the 405 patches (centred complex
+    SVD, hard threshold, synthesis, weighted accumulation), both timed.
+    Returns (seconds, voxel-frames the step stands for = the call's / 5)."""
     from oracle import oracle as O
 
     p_s, p_o = O.patch_params(x.shape, PATCH, OVERLAP)
     ps, step, grid = O.grid_geometry(x.shape, p_s, p_o)
-    rng = np.random.RandomState(1)
-    t0 = time.perf_counter()
-    mcs = oracle.nordic_threshold(p_s, x.shape[-1], NOISE, mc_draws, rng)
-    t_mc = (time.perf_counter() - t0) * (N_ITER / mc_draws)
-    thr = float(mcs)
     n_all = int(np.prod(grid))
+    draws, n_patches = N_ITER // SAMPLE_FRACTION, n_all // SAMPLE_FRACTION
+    assert draws * SAMPLE_FRACTION == N_ITER and n_patches * SAMPLE_FRACTION == n_all
+    rng = np.random.RandomState(1)
     out = np.zeros(x.shape, np.complex64)
     w = np.zeros(x.shape, np.float32)
     t0 = time.perf_counter()
+    thr = float(O.nordic_threshold(p_s, x.shape[-1], NOISE, draws, rng))
     for i in range(n_patches):
         sl = O._patch_slices(i, ps, step, grid)
         patch = x[sl].reshape(int(np.prod(p_s[:-1])), -1)
@@ -134,33 +134,48 @@ def cpu_reference_sample(x, mc_draws=1, n_patches=60):
         theta = 1 / (2 + rank)
         out[sl] += new.reshape(ps) * theta
         w[sl] += theta
-    t_p = (time.perf_counter() - t0) * (n_all / n_patches)
-    desc = (f"{mc_draws} of {N_ITER} Monte-Carlo SVDs and {n_patches} of {n_all} patches of the complex64 volume, "
-            f"scaled to the full call")
-    return t_mc + t_p, desc
+    return time.perf_counter() - t0, float(np.prod(SHAPE)) / SAMPLE_FRACTION
+
+
+def cpu_full_call(x):
+    """The CPU oracle's whole NORDIC call on the benchmarked volume (10 Monte-Carlo
+    SVDs, all 405 patches, normalisation). Returns seconds."""
+    import oracle
+
+    t0 = time.perf_counter()
+    oracle.denoise("nordic", x, PATCH, OVERLAP, recombination="weighted", noise_std=NOISE,
+                   n_iter_threshold=N_ITER, nordic_rng=np.random.RandomState(1))
+    return time.perf_counter() - t0
+
+
+def bench_config(precision):
+    """The ``config`` both arms print (the same keys and values)."""
+    return {"workload": WORKLOAD, "precision": precision, "parallelism": "replicas",
+            "l2": "input 262 MB > 126 MB L2 per step (no flush)"}
 
 
 def reference_arm(args, rank, world):
     if rank != 0:
         return
     x = make_volume()
-    vf = float(np.prod(SHAPE))
     for _ in range(args.warmup):
-        cpu_reference_sample(x)
-    times = []
-    desc = ""
+        cpu_sample_step(x)
+    secs, vfs = [], 0.0
     for _ in range(args.steps):
-        t, desc = cpu_reference_sample(x)
-        times.append(t)
-    t = float(np.mean(times))
-    val = vf / t
+        t, vf = cpu_sample_step(x)
+        secs.append(t)
+        vfs += vf
+    t = float(np.sum(secs))
+    val = vfs / t
     cores = os.cpu_count()
+    sample = (f"each step: 2 of the 10 Monte-Carlo SVDs (266200 x 200) and 81 of the 405 patches, exactly "
+              f"1/{SAMPLE_FRACTION} of one call, timed; value = the steps' voxel-frames / their time")
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "voxel-frames/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64 patch SVDs, f64 Monte-Carlo SVDs", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "impl": "CPU oracle (reference algorithm, NumPy/SciPy LAPACK)"},
-        "cpu_baseline": {"value": val, "unit": "voxel-frames/s", "cores": cores, "kind": "port", "sample": desc},
+        "config": bench_config(args.precision),
+        "cpu_baseline": {"value": val, "unit": "voxel-frames/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": val, "unit": "voxel-frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -168,35 +183,38 @@ def reference_arm(args, rank, world):
 
 # --------------------------------------------------------------------------- GPU arm
 def algorithmic(kernel, n_patches, M, n, ranks):
-    """(algorithmic work per call, "flop" or "byte") of a library kernel for this workload (complex64)."""
+    """(algorithmic work per call, "flop" or "byte") of a library kernel for this
+    workload (complex64). Bytes count one read of the input and one write of the
+    outputs a kernel owns; patch-overlap re-reads and the intermediates the
+    mixed path writes and re-reads (bf16 operands, Gaussian draws) are traffic,
+    not algorithmic work."""
     P = n_patches
+    vol = 8.0 * float(np.prod(SHAPE))  # complex64 volume bytes
     if kernel in ("gram_fp32", "gram_tc"):
         return 4.0 * M * n * (n + 1) * P, "flop"  # complex Hermitian rank-M update, lower triangle
     if kernel in ("mc_gram", "mc_gram_tc"):
         return float(N_ITER) * M * n * n * (n + 1), "flop"  # draws of (M n) x n, lower triangle
     if kernel == "eig":
         return 16.0 / 3.0 * n**3 * P, "flop"  # complex Householder tridiagonalisation
+    if kernel == "eig_sub8":
+        # 4 block products C Q (8 n^2 FLOP per complex column, 8 columns) per patch
+        return 4.0 * 8.0 * n * n * 8 * P, "flop"
     if kernel == "synth_scatter":
-        return 8.0 * M * n * P + 8.0 * M * n * P, "byte"  # complex rows in; theta-scaled rows scattered (atomics)
+        return 2.0 * vol, "byte"  # the volume read once, the output written once
     if kernel == "finalize":
         return (8.0 + 8.0 + 4.0 + 4.0) * float(np.prod(SHAPE)), "byte"  # out read + written, weights, noise map
-    if kernel == "gauss_pack":
-        return 2.0 * N_ITER * M * n * n, "byte"  # bf16 normals written
-    if kernel == "pack":
-        return 8.0 * M * n * P + 8.0 * M * n * P, "byte"  # complex rows in; bf16 hi and lo of the M x 2n real embedding out
-    if kernel == "patch_mean":
-        return 8.0 * M * n * P, "byte"
+    if kernel in ("pack", "patch_mean"):
+        return vol, "byte"  # the volume read once
     return None, None
 
 
-# DRAM bytes per launch from the ncu captures summarised under profiles/
-# (dram__bytes_read.sum + dram__bytes_write.sum of one launch).
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
+# separate ncu capture of each kernel on this workload; they are not measured in
+# the timed run.
 NCU_TRAFFIC = {
-    "eig": 65.277e6 + 0.140e6,  # profiles/k_eig_c64_n200_405patches.md
-    "mc_gram_tc": 1.075e9 + 0.106e9,  # profiles/k_gram_tma_mc_draws_10x266200x200.md
-    "gauss_pack": 0.025e6 + 1.007e9,  # profiles/k_gauss_pack_10x266200x200.md
-    "eig_mc": 0.846e6,  # profiles/k_top1_mc_draws_10x200.md
-    # profiles/dram_traffic_pack_gram_synth_finalize_c64_64x64x40x200.md
+    "mc_gram_tc": 1.075e9 + 0.106e9,
+    "gauss_pack": 0.025e6 + 1.007e9,
+    "eig_mc": 0.846e6,
     "pack": 0.310e9 + 0.811e9,
     "gram_tc": 0.871e9 + 0.059e9,
     "synth_scatter": 0.392e9 + 0.150e9,
@@ -226,7 +244,8 @@ def roofline(name, per_launch_ms, launches, steps, work, kind, peaks):
         src = f"nominal FP32 CUDA-core peak, 148 SMs x 128 lanes x 2 FLOP x {mhz:.0f} MHz (no measured FP32 figure)"
     tr = NCU_TRAFFIC.get(name)
     return {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-            "frac": achieved / peak, "traffic": tr, "algorithmic_per_launch": per_launch,
+            "frac": achieved / peak, "traffic": tr,
+            "traffic_source": "separate ncu capture (DRAM read + write bytes per launch)" if tr else None, "algorithmic_per_launch": per_launch,
             "algorithmic_unit": "FLOP" if kind == "flop" else "byte", "peak_source": src,
             "per_launch_ms": per_launch_ms, "launches": launches}
 
@@ -386,8 +405,7 @@ def ours_arm(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if precision == "fp32" else "bf16+f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "precision": precision, "parallelism": f"replicas x{world}",
-                       "l2": "input 262 MB > 126 MB L2 per step (no flush)"},
+            "config": bench_config(precision),
             "plain_fp32": {"value": world * vf / (ms_fp32 * 1e-3), "ms_per_step": ms_fp32,
                            "speedup_chosen": ms_fp32 / ms, "rel_l2_chosen_vs_plain": rel_err},
             "e2e": {"value": world * vf / (e2e_ms * 1e-3), "unit": "voxel-frames/s", "h2d_bytes_per_step": h2d,
@@ -406,9 +424,11 @@ def ours_arm(args, rank, world):
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu:
-            t_cpu, desc = cpu_reference_sample(x)
+            t_cpu = cpu_full_call(x)
             line["cpu_baseline"] = {"value": vf / t_cpu, "unit": "voxel-frames/s", "cores": os.cpu_count(),
-                                    "kind": "port", "sample": desc}
+                                    "kind": "port", "seconds": t_cpu,
+                                    "sample": "one whole call of the CPU oracle on the benchmarked volume (10 "
+                                              "Monte-Carlo SVDs, 405 patches), NumPy/SciPy LAPACK on all host cores"}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
