@@ -249,6 +249,31 @@ pd_status pd_denoise_patches_noalloc(const pd_geometry* g, const pd_params* p, c
  * PD_ERR_CUDA if a bounded device-side wait timed out, PD_OK otherwise. */
 pd_status pd_noalloc_check(void* stream);
 
+/* Scratch bytes pd_lowrank_backward needs for n_selected patches. */
+pd_status pd_lowrank_backward_workspace_size(const pd_geometry* g, int64_t n_selected, size_t* bytes);
+
+/* Gradient of the low-rank patch denoiser with respect to its input and its
+ * threshold (real float32 volumes, weighted or average recombination). The
+ * reference has no gradient; this is the adjoint of its forward path
+ * (BaseSpaceTimeDenoiser.denoise, space_time/base.py:177-270) with the shrinkage
+ *   shrink 0: soft threshold s~ = max(s - tau_p, 0), tau_p = stdest_p * level,
+ *             stdest_p = sqrt(mean over the patch of noise_std^2) (the adaptive
+ *             trace-norm shrinkage of space_time/lowrank.py:459-461 at gamma 1);
+ *   shrink 1: hard threshold at the forward's rank (MP-PCA / hybrid / raw rules
+ *             at a fixed decision; the threshold gradient is then zero).
+ * Every patch's factorisation is recomputed (mean, Gram, all eigenpairs).
+ *   d_in, d_patch_list, d_patch_rank  the forward's input, patch list and maxidx
+ *   d_weights   the forward's 4D float32 weights (recombination normaliser)
+ *   d_gout      upstream gradient, the input's shape
+ *   d_gin       gradient with respect to the input, zeroed by the caller (accumulated)
+ *   d_dlevel    float64 [n_selected]: each patch's dL/dlevel (0 for shrink 1)
+ * Needs more voxels than frames per patch and at most 128 frames. */
+pd_status pd_lowrank_backward(const pd_geometry* g, int32_t recombination, int32_t shrink, const float* d_in,
+                              const double* d_noise_std, double level, const int32_t* d_patch_list,
+                              int64_t n_selected, const int32_t* d_patch_rank, const float* d_weights,
+                              const float* d_gout, float* d_gin, double* d_dlevel, void* d_workspace,
+                              size_t workspace_bytes, void* stream);
+
 /* Scratch bytes pd_estimate_noise needs (shape as for pd_estimate_noise). */
 pd_status pd_estimate_noise_workspace_size(int32_t ndim, const int64_t* shape, int32_t is_complex, size_t* bytes);
 

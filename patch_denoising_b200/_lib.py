@@ -108,6 +108,11 @@ SIGNATURES = {
         [G_P, P_P, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     ),
     "pd_noalloc_check": (c_i32, [c_vp]),
+    "pd_lowrank_backward_workspace_size": (c_i32, [G_P, c_i64, ctypes.POINTER(c_sz)]),
+    "pd_lowrank_backward": (
+        c_i32,
+        [G_P, c_i32, c_i32, c_vp, c_vp, c_dbl, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_sz, c_vp],
+    ),
     "pd_estimate_noise_workspace_size": (c_i32, [c_i32, ctypes.POINTER(c_i64), c_i32, ctypes.POINTER(c_sz)]),
     "pd_estimate_noise": (c_i32, [c_i32, ctypes.POINTER(c_i64), c_i32, c_vp, c_i32, c_vp, c_vp, c_sz, c_vp]),
     "pd_workspace_check": (c_i32, [c_vp, c_vp]),

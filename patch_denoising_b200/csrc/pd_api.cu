@@ -571,6 +571,97 @@ pd_status pd_adaptive_denoise_patches(const pd_geometry* g, const pd_params* p, 
                               stream, nullptr, a);
 }
 
+// ---------------------------------------------------------------------------
+// Backward pass of the low-rank denoiser (real volumes)
+// ---------------------------------------------------------------------------
+static size_t bwd_extra_bytes(int count, int n) {
+  Carver c(nullptr);
+  c.take<float>((size_t)count * n * n);  // cross
+  c.take<float>((size_t)count * n * n);  // k1
+  c.take<float>((size_t)count * n * n);  // k2
+  c.take<float>((size_t)count * n);      // gmean
+  c.take<float>((size_t)count * n);      // u
+  return c.off;
+}
+
+static pd_status check_backward(const pd_geometry* g, int32_t recombination, int32_t shrink) {
+  PD_TRY(check_geometry(g));
+  if (recombination != PD_RECOMB_WEIGHTED && recombination != PD_RECOMB_AVERAGE)
+    return fail(PD_ERR_INVALID, "the backward pass needs 'weighted' or 'average' recombination");
+  if (shrink != 0 && shrink != 1) return fail(PD_ERR_INVALID, "shrink must be 0 (soft) or 1 (hard)");
+  if (!bwd_supported((int)g->cols))
+    return fail(PD_ERR_UNSUPPORTED, "the backward pass handles at most 128 frames per patch (got %lld)",
+                (long long)g->cols);
+  if (g->rows <= g->cols)
+    return fail(PD_ERR_UNSUPPORTED, "the backward pass needs more voxels than frames per patch (M > T)");
+  return PD_OK;
+}
+
+pd_status pd_lowrank_backward_workspace_size(const pd_geometry* g, int64_t n_selected, size_t* bytes) {
+  g_err.clear();
+  PD_TRY(check_backward(g, PD_RECOMB_AVERAGE, 0));
+  if (!bytes) return fail(PD_ERR_INVALID, "NULL output");
+  const int n = (int)g->cols;
+  const size_t pp = per_patch_bytes(n, false) + (size_t)3 * n * n * 4 + (size_t)2 * n * 4 + 5 * 256;
+  int64_t chunk = (int64_t)std::max<size_t>(1, DEFAULT_CHUNK_BUDGET / pp);
+  chunk = std::min<int64_t>(chunk, std::max<int64_t>(n_selected, 1));
+  *bytes = work_bytes((int)chunk, n, false) + bwd_extra_bytes((int)chunk, n);
+  return PD_OK;
+}
+
+pd_status pd_lowrank_backward(const pd_geometry* g, int32_t recombination, int32_t shrink, const float* d_in,
+                              const double* d_noise_std, double level, const int32_t* d_patch_list,
+                              int64_t n_selected, const int32_t* d_patch_rank, const float* d_weights,
+                              const float* d_gout, float* d_gin, double* d_dlevel, void* d_ws, size_t ws_bytes,
+                              void* stream) {
+  g_err.clear();
+  PD_TRY(check_backward(g, recombination, shrink));
+  if (n_selected == 0) return PD_OK;
+  if (!d_in || !d_patch_list || !d_patch_rank || !d_weights || !d_gout || !d_gin || !d_dlevel)
+    return fail(PD_ERR_INVALID, "NULL buffer");
+  if (shrink == 0 && !d_noise_std) return fail(PD_ERR_INVALID, "the soft threshold needs the noise_std map");
+  const int n = (int)g->cols;
+  const size_t one = work_bytes(1, n, false) + bwd_extra_bytes(1, n);
+  if (!d_ws || ws_bytes < one) return fail(PD_ERR_WORKSPACE, "workspace too small (%zu < %zu)", ws_bytes, one);
+  // per-patch bytes without the alignment slack: an upper bound on the chunk
+  const size_t pp = per_patch_bytes(n, false) + (size_t)3 * n * n * 4 + (size_t)2 * n * 4;
+  int64_t chunk = std::min<int64_t>(n_selected, std::max<int64_t>(1, (int64_t)(ws_bytes / pp)));
+  while (chunk > 1 && work_bytes((int)chunk, n, false) + bwd_extra_bytes((int)chunk, n) > ws_bytes) --chunk;
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geo G = to_geo(*g);
+  EigParams ep{};
+  ep.method = EIG_MODE_FULL;
+  ep.rows = (int)g->rows;
+  ep.cols = n;
+  PD_TRY(cuda_check(cudaMemsetAsync(d_ws, 0, sizeof(int), s), "clear error word"));
+  for (int64_t off = 0; off < n_selected; off += chunk) {
+    const int cnt = (int)std::min<int64_t>(chunk, n_selected - off);
+    size_t used;
+    PatchWork w = carve_work(d_ws, cnt, n, false, &used);
+    w.list = d_patch_list + off;
+    Carver c((char*)d_ws + used);
+    BwdWork b{};
+    b.recombination = recombination;
+    b.shrink = shrink;
+    b.level = level;
+    b.rank = d_patch_rank + off;
+    b.cross = c.take<float>((size_t)cnt * n * n);
+    b.k1 = c.take<float>((size_t)cnt * n * n);
+    b.k2 = c.take<float>((size_t)cnt * n * n);
+    b.mat_stride = (int64_t)n * n;
+    b.gmean = c.take<float>((size_t)cnt * n);
+    b.u = c.take<float>((size_t)cnt * n);
+    b.dlevel = d_dlevel + off;
+    // the forward's factorisation, recomputed in FP32: mean, Gram, every eigenpair
+    launch_patch_mean(G, false, d_in, w, s);
+    if (shrink == 0) launch_prior(G, PD_METHOD_ADAPTIVE, d_noise_std, w, s);
+    launch_gram_fp32(G, false, d_in, w, s);
+    PD_TRY(cuda_check(launch_eig(false, n, ep, w, s), "eigensolver launch"));
+    PD_TRY(cuda_check(launch_backward(G, d_in, d_gout, d_weights, d_gin, w, b, s), "backward launch"));
+  }
+  return PD_OK;
+}
+
 // Spatial extents padded to 3 axes (block 1 on padded axes) and frame count.
 static pd_status noise_geometry(int32_t ndim, const int64_t* shape, int32_t block, int64_t dims[3], int blk[3],
                                 int* frames) {

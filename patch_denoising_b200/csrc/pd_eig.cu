@@ -868,7 +868,18 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
   const double M = (double)ep.rows, pt = (double)ep.cols;
 
   // ---------------------------------------------------------------- decisions
-  if (ADAPT && ep.method == PD_METHOD_ADAPTIVE) {  // compiled into the ADAPT instantiation only
+  if (ADAPT && ep.method == EIG_MODE_FULL) {  // the whole decomposition (ADAPT instantiation)
+    for (int i = tid; i < n; i += EIG_THREADS) idx[i] = i;
+    __syncthreads();
+    cta_eigs(d, e2, n, ti, idx, lam, n);
+    for (int a = tid; a < n; a += EIG_THREADS) {
+      aidx[a] = n - 1 - a;
+      alam[a] = lam[n - 1 - a];
+      acoef[a] = (float)((double)lam[n - 1 - a] * tscale);
+    }
+    if (tid == 0) s_act = n;
+    __syncthreads();
+  } else if (ADAPT && ep.method == PD_METHOD_ADAPTIVE) {  // compiled into the ADAPT instantiation only
     adaptive_rule(ep, ad, w, p, n, d, e2, ti, idx, lam, aidx, alam, acoef, reinterpret_cast<double*>(pw), tscale, M,
                   pt, &s_act);
   } else if (ep.method == PD_METHOD_MPPCA || ep.method == PD_METHOD_HYBRID) {
@@ -1275,7 +1286,8 @@ static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaSt
       flags |= 2;
     }
   }
-  auto kern = ep.method == PD_METHOD_ADAPTIVE ? k_eig<CPLX, NS, true> : k_eig<CPLX, NS, false>;
+  auto kern = (ep.method == PD_METHOD_ADAPTIVE || ep.method == EIG_MODE_FULL) ? k_eig<CPLX, NS, true>
+                                                                               : k_eig<CPLX, NS, false>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   pd_adaptive a{};

@@ -49,7 +49,7 @@ void launch_gram_fp32(const Geo& g, bool cplx, const void* in, const PatchWork& 
 
 // pd_eig.cu
 struct EigParams {
-  int method;  // PD_METHOD_* or EIG_MODE_TOP1 (MC threshold)
+  int method;  // PD_METHOD_*, EIG_MODE_TOP1 (MC threshold) or EIG_MODE_FULL
   int loss;
   int has_prior;
   int rows;  // M
@@ -61,6 +61,9 @@ struct EigParams {
   int only_unfinished;        // 1: solve only the patches with n_active < 0 (left by k_sub)
 };
 constexpr int EIG_MODE_TOP1 = 100;
+// every eigenpair, descending: vectors into w.vec, eigenvalues (true units) into
+// w.coef, n_active = n (the backward pass's factorisation)
+constexpr int EIG_MODE_FULL = 101;
 cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s,
                        const pd_adaptive* ad = nullptr);
 size_t eig_smem_bytes(bool cplx, int n, bool* in_smem);
@@ -87,6 +90,24 @@ void launch_synth(const Geo& g, bool cplx, const void* in, const PatchWork& w, c
 void launch_finalize(const Geo& g, bool cplx, int recombination, void* out, const float* weight_acc,
                      const float* noise_acc, const float* noise_ctr, float* weights, float* noise_map,
                      const uint8_t* mask, int mask_is_4d, cudaStream_t s);
+
+// pd_backward.cu: adjoint of the low-rank patch denoiser (real volumes)
+struct BwdWork {
+  int recombination;    // PD_RECOMB_WEIGHTED or PD_RECOMB_AVERAGE
+  int shrink;           // 0 soft threshold at stdest * level, 1 hard at the patch rank
+  double level;         // soft: tau_p = stdest_p * level
+  const int32_t* rank;  // [count] the forward's maxidx per patch
+  float* cross;         // [count][mat_stride] Xc^T Gb
+  float* k1;            // [count][mat_stride] V E V^T
+  float* k2;            // [count][mat_stride] V diag(h/s) V^T
+  int64_t mat_stride;   // floats per patch (n * n)
+  float* gmean;         // [count][n] mean row of Gb
+  float* u;             // [count][n] gmean (I - K2)
+  double* dlevel;       // [count] dL/dlevel per patch (soft), 0 (hard)
+};
+bool bwd_supported(int n);
+cudaError_t launch_backward(const Geo& g, const float* in, const float* gout, const float* wts, float* gin,
+                            const PatchWork& w, const BwdWork& b, cudaStream_t s);
 
 // pd_gram_tma.cu (pack + TMA-fed tcgen05)
 size_t packed_bytes_per_patch(int n, bool cplx, int M);

@@ -1,6 +1,7 @@
 """Space-time denoisers (drop-in for ``patch_denoise.space_time``)."""
 
 from .base import BaseSpaceTimeDenoiser, PatchedArray
+from .diff import LowRankDenoiseFunction, LowRankDenoiseLayer, lowrank_denoise, mc_sure, sure_tune_threshold
 from .lowrank import (
     AdaptiveDenoiser,
     HybridPCADenoiser,
@@ -35,4 +36,9 @@ __all__ = [
     "svd_synthesis",
     "eig_analysis",
     "eig_synthesis",
+    "LowRankDenoiseFunction",
+    "LowRankDenoiseLayer",
+    "lowrank_denoise",
+    "mc_sure",
+    "sure_tune_threshold",
 ]
