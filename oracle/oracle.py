@@ -399,6 +399,7 @@ def atn_cost64(s, si, x_shape, lt, gamma, sigma, gsure):
     the form the library evaluates on the device."""
     n_rows, n_cols = x_shape
     tau = np.exp(lt)
+    s, si = s[s > 0], si[s > 0]  # zero singular values add nothing (their terms vanish as s -> 0)
     r = np.exp(gamma * (lt - np.log(s)))
     d_hat = s * np.maximum(1 - r, 0)
     div = np.sum((1 + (gamma - 1) * r) * (s >= tau) + abs(n_rows - n_cols) * d_hat / s) + 2 * np.sum(s * d_hat * si)
@@ -498,9 +499,14 @@ def _adaptive_patch(x, stdest, method, gamma0, tau0, nbsim, qlevel=None, rng=Non
     u, s, vt, mean = svd_analysis(x)
     if optimizer == "search":
         s = s.astype(np.float64)  # the cost in float64 whatever the patch's precision
+        if x.shape[0] <= x.shape[1]:
+            # a centred M x T patch with M <= T has rank M - 1 at most: its last
+            # singular values are zero (rounding leaves them tiny), as the library takes them
+            s = s.copy()
+            s[x.shape[0] - 1 :] = 0.0
         s2 = s**2
         with np.errstate(divide="ignore"):
-            si = np.array([np.sum(1.0 / (s2[k] - np.delete(s2, k))) for k in range(len(s))])
+            si = np.array([np.sum(1.0 / (s2[k] - np.delete(s2, k))) if s[k] > 0 else 0.0 for k in range(len(s))])
         gs = method == "gsure"
         if method == "qut":
             tau = stdest * qlevel
@@ -511,8 +517,10 @@ def _adaptive_patch(x, stdest, method, gamma0, tau0, nbsim, qlevel=None, rng=Non
                 gamma = np.exp(line_search_min(lambda g: atn_cost64(s, si, x.shape, lt, np.exp(g) + 1, stdest, gs),
                                                0.0)) + 1
         else:
-            x0 = np.log(np.median(s)) if tau0 is None else tau0
-            lo, hi = np.log(s[-1]) - 10.0, np.log(s[0]) + 10.0  # the library's bounds on log tau
+            pos = s[s > 0]
+            med = np.median(s)
+            x0 = (np.log(med) if med > 0 else np.log(pos[-1]) - 10.0) if tau0 is None else tau0
+            lo, hi = np.log(pos[-1]) - 10.0, np.log(s[0]) + 10.0  # the library's bounds on log tau
             best = np.inf
             gamma, tau = gamma0[0], np.exp(x0)
             for g in gamma0:

@@ -687,8 +687,11 @@ __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adap
   double* sv = scratch;
   double* lsv = sv + n;
   double* si = lsv + n;
+  // a centred M x T patch with M <= T has rank M - 1 at most: its singular
+  // values from index M - 1 on are zero (the Gram's rounding leaves them small)
+  const int nz = ep.rows <= n ? ep.rows - 1 : nv;
   for (int k = tid; k < nv; k += EIG_THREADS) {
-    sv[k] = sqrt(fmax((double)lam[n - 1 - k] * tscale, 0.0));
+    sv[k] = k < nz ? sqrt(fmax((double)lam[n - 1 - k] * tscale, 0.0)) : 0.0;
     lsv[k] = log(sv[k]);
   }
   __syncthreads();

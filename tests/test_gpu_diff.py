@@ -81,9 +81,9 @@ def _torch_reference(x, scale, nmap, shrink, recombination, ranks=None):
     return (acc / W).reshape(x.shape)
 
 
-def _mp_ranks(x):
+def _mp_ranks(x, scale):
     res = _engine.run("mp-pca", torch.from_numpy(x).to(DEV), (PATCH,) * 3 + (SHAPE[-1],),
-                      (OVERLAP,) * 3 + (SHAPE[-1],), "weighted", None, 50, threshold_scale=1.0)
+                      (OVERLAP,) * 3 + (SHAPE[-1],), "weighted", None, 50, threshold_scale=scale)
     return res.patch_rank.long()
 
 
@@ -103,7 +103,7 @@ def test_gradients_match_torch_svd_autograd(shrink, recombination):
     # FP64 torch reference
     x64 = torch.from_numpy(x.astype(np.float64)).to(DEV).requires_grad_(True)
     s64 = torch.tensor(scale, dtype=torch.float64, device=DEV, requires_grad=True)
-    ranks = _mp_ranks(x) if shrink == "hard" else None
+    ranks = _mp_ranks(x, scale) if shrink == "hard" else None
     ref = _torch_reference(x64, s64, torch.from_numpy(nmap).to(DEV), shrink, recombination, ranks)
     np.testing.assert_array_equal(torch.isfinite(ref).cpu().numpy(), fin.cpu().numpy())
     rl = (torch.where(torch.isfinite(ref), ref, torch.zeros_like(ref)) * w).sum()
