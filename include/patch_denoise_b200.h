@@ -249,6 +249,51 @@ pd_status pd_denoise_patches_noalloc(const pd_geometry* g, const pd_params* p, c
  * PD_ERR_CUDA if a bounded device-side wait timed out, PD_OK otherwise. */
 pd_status pd_noalloc_check(void* stream);
 
+/* One volume of a batched call: its geometry, device buffers (as for
+ * pd_denoise_patches) and per-volume rule parameters. */
+typedef struct pd_volume {
+  pd_geometry geometry;
+  const void* d_in;           /* float32 or complex64 volume                       */
+  const double* d_noise_std;  /* spatial noise_std map when the method needs one   */
+  const int32_t* d_patch_list; /* the volume's selected patches (pd_select_patches) */
+  int64_t n_selected;
+  void* d_out_acc;
+  float* d_weight_acc;
+  float* d_noise_acc;
+  float* d_noise_ctr;
+  int32_t* d_rank_map;
+  int32_t* d_patch_rank;      /* [n_selected]                                      */
+  float* d_patch_noise;       /* [n_selected]                                      */
+  double threshold;           /* raw: the singular-value threshold                 */
+  double mp_median;           /* optimal: Marchenko-Pastur median of T / M         */
+} pd_volume;
+
+#define PD_BATCH_MAX_VOLUMES 64
+
+/* Launch-shape choices of a batched call (an autotuner picks them by timing). */
+typedef struct pd_batch_tuning {
+  int32_t synth_row_blocks; /* CTAs per patch in the synthesis scatter; 0 = by the patch's rows */
+  int32_t order_by_cost;    /* 1: volumes in descending per-patch cost order (frames^3), 0: as given */
+  int64_t chunk_patches;    /* patches per launch; 0 = as many as the workspace holds */
+} pd_batch_tuning;
+
+/* Scratch bytes pd_denoise_batch needs (chunk_patches as in pd_batch_tuning). */
+pd_status pd_denoise_batch_workspace_size(const pd_volume* vols, int32_t n_vols, const pd_params* p,
+                                          int64_t chunk_patches, size_t* bytes);
+
+/* pd_denoise_patches over up to PD_BATCH_MAX_VOLUMES volumes of uneven shape in
+ * one set of launches: the volumes' selected patches form one work list (its
+ * order by tuning->order_by_cost), and every patch kernel reads its patch's
+ * volume (geometry, buffers, threshold / MP median) from a device table, so a
+ * launch spans every volume. Plain FP32 kernels; methods MP-PCA, hybrid, raw and
+ * optimal (p->threshold and p->mp_median are taken per volume). No reference
+ * counterpart: the reference denoises one volume per call (base.py:177-270) and
+ * its GPU module batches the patches of one volume (gpu/main.py:186-244).
+ * Normalise each volume with pd_finalize afterwards. tuning may be NULL. */
+pd_status pd_denoise_batch(const pd_volume* vols, int32_t n_vols, const pd_params* p,
+                           const pd_batch_tuning* tuning, void* d_workspace, size_t workspace_bytes,
+                           void* stream);
+
 /* Scratch bytes pd_lowrank_backward needs for n_selected patches. */
 pd_status pd_lowrank_backward_workspace_size(const pd_geometry* g, int64_t n_selected, size_t* bytes);
 

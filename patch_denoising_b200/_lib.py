@@ -73,6 +73,35 @@ class Adaptive(ctypes.Structure):
     ]
 
 
+class Volume(ctypes.Structure):
+    """``pd_volume``."""
+
+    _fields_ = [
+        ("geometry", Geometry),
+        ("d_in", c_vp),
+        ("d_noise_std", c_vp),
+        ("d_patch_list", c_vp),
+        ("n_selected", c_i64),
+        ("d_out_acc", c_vp),
+        ("d_weight_acc", c_vp),
+        ("d_noise_acc", c_vp),
+        ("d_noise_ctr", c_vp),
+        ("d_rank_map", c_vp),
+        ("d_patch_rank", c_vp),
+        ("d_patch_noise", c_vp),
+        ("threshold", c_dbl),
+        ("mp_median", c_dbl),
+    ]
+
+
+class BatchTuning(ctypes.Structure):
+    """``pd_batch_tuning``."""
+
+    _fields_ = [("synth_row_blocks", c_i32), ("order_by_cost", c_i32), ("chunk_patches", c_i64)]
+
+
+BATCH_MAX_VOLUMES = 64
+
 G_P = ctypes.POINTER(Geometry)
 P_P = ctypes.POINTER(Params)
 A_P = ctypes.POINTER(Adaptive)
@@ -108,6 +137,8 @@ SIGNATURES = {
         [G_P, P_P, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     ),
     "pd_noalloc_check": (c_i32, [c_vp]),
+    "pd_denoise_batch_workspace_size": (c_i32, [ctypes.POINTER(Volume), c_i32, P_P, c_i64, ctypes.POINTER(c_sz)]),
+    "pd_denoise_batch": (c_i32, [ctypes.POINTER(Volume), c_i32, P_P, ctypes.POINTER(BatchTuning), c_vp, c_sz, c_vp]),
     "pd_lowrank_backward_workspace_size": (c_i32, [G_P, c_i64, ctypes.POINTER(c_sz)]),
     "pd_lowrank_backward": (
         c_i32,

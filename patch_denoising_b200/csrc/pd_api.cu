@@ -82,6 +82,7 @@ PatchWork carve_work(void* ws, int count, int n, bool cplx, size_t* used, size_t
   PatchWork w{};
   w.err = c.take<int>(1);  // always at offset 0 of the workspace
   w.count = count;
+  w.n_stride = n;
   w.packed = packed_per_patch ? (void*)c.take<uint8_t>(packed_per_patch * count) : nullptr;
   w.mean = c.take<float>((size_t)count * n * (cplx ? 2 : 1));
   w.gram_stride = gram_stride_floats(n, cplx);
@@ -399,6 +400,7 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
     sa.patch_noise = d_patch_noise;
     sa.list_offset = off;
     sa.wide = p->method == PD_METHOD_ADAPTIVE ? 1 : 0;
+    sa.row_blocks = 0;
     launch_synth(G, cplx, d_in, w, sa, s);
     PD_TRY(cuda_check(cudaGetLastError(), "pd_denoise_patches launch"));
   }
@@ -569,6 +571,149 @@ pd_status pd_adaptive_denoise_patches(const pd_geometry* g, const pd_params* p, 
   return denoise_patches_impl(g, p, d_in, d_noise_std, d_patch_list, n_selected, d_out_acc, d_weight_acc,
                               d_noise_acc, d_noise_ctr, d_rank_map, d_patch_rank, d_patch_noise, d_ws, ws_bytes,
                               stream, nullptr, a);
+}
+
+// ---------------------------------------------------------------------------
+// Batched calls over many volumes
+// ---------------------------------------------------------------------------
+static pd_status batch_check(const pd_volume* vols, int32_t n_vols, const pd_params* p, int* n_max, int* m_max,
+                             int64_t* total) {
+  if (!vols || n_vols < 1) return fail(PD_ERR_INVALID, "no volumes");
+  if (n_vols > PD_BATCH_MAX_VOLUMES)
+    return fail(PD_ERR_UNSUPPORTED, "at most %d volumes per batch", PD_BATCH_MAX_VOLUMES);
+  if (!p) return fail(PD_ERR_INVALID, "params is NULL");
+  if (p->precision != PD_PRECISION_FP32) return fail(PD_ERR_UNSUPPORTED, "batched calls run the FP32 kernels");
+  if (p->method == PD_METHOD_ADAPTIVE) return fail(PD_ERR_UNSUPPORTED, "batched calls take MP-PCA, hybrid, raw, optimal");
+  *n_max = 0;
+  *m_max = 0;
+  *total = 0;
+  for (int v = 0; v < n_vols; ++v) {
+    PD_TRY(check_geometry(&vols[v].geometry));
+    PD_TRY(check_params(&vols[v].geometry, p));
+    if (vols[v].n_selected < 0) return fail(PD_ERR_INVALID, "negative patch count");
+    *n_max = std::max(*n_max, (int)vols[v].geometry.cols);
+    *m_max = std::max(*m_max, (int)vols[v].geometry.rows);
+    *total += vols[v].n_selected;
+  }
+  return PD_OK;
+}
+
+static size_t batch_table_bytes(int32_t n_vols, int64_t total) {
+  return align256(sizeof(VolDesc) * n_vols) + 2 * align256(sizeof(int32_t) * std::max<int64_t>(total, 1));
+}
+
+pd_status pd_denoise_batch_workspace_size(const pd_volume* vols, int32_t n_vols, const pd_params* p,
+                                          int64_t chunk_patches, size_t* bytes) {
+  g_err.clear();
+  int n_max, m_max;
+  int64_t total;
+  PD_TRY(batch_check(vols, n_vols, p, &n_max, &m_max, &total));
+  if (!bytes) return fail(PD_ERR_INVALID, "NULL output");
+  const bool cplx = p->is_complex != 0;
+  int64_t chunk = (int64_t)std::max<size_t>(1, DEFAULT_CHUNK_BUDGET / per_patch_bytes(n_max, cplx));
+  if (chunk_patches > 0) chunk = std::min(chunk, chunk_patches);
+  chunk = std::min<int64_t>(chunk, std::max<int64_t>(total, 1));
+  *bytes = work_bytes((int)chunk, n_max, cplx) + batch_table_bytes(n_vols, total);
+  return PD_OK;
+}
+
+pd_status pd_denoise_batch(const pd_volume* vols, int32_t n_vols, const pd_params* p, const pd_batch_tuning* tuning,
+                           void* d_ws, size_t ws_bytes, void* stream) {
+  g_err.clear();
+  int n_max, m_max;
+  int64_t total;
+  PD_TRY(batch_check(vols, n_vols, p, &n_max, &m_max, &total));
+  const bool cplx = p->is_complex != 0;
+  for (int v = 0; v < n_vols; ++v) {
+    const pd_volume& vv = vols[v];
+    if (vv.n_selected > 0 && (!vv.d_in || !vv.d_patch_list || !vv.d_out_acc || !vv.d_weight_acc ||
+                              !vv.d_noise_acc || !vv.d_noise_ctr || !vv.d_rank_map || !vv.d_patch_rank ||
+                              !vv.d_patch_noise))
+      return fail(PD_ERR_INVALID, "NULL buffer in volume %d", v);
+    if ((p->method == PD_METHOD_HYBRID || (p->method == PD_METHOD_OPTIMAL && p->has_prior)) && !vv.d_noise_std)
+      return fail(PD_ERR_INVALID, "volume %d needs its noise_std map", v);
+  }
+  if (total == 0) return PD_OK;
+  pd_batch_tuning tn{};
+  tn.order_by_cost = 1;
+  if (tuning) tn = *tuning;
+  // work-list order: the costliest patches (eigensolver ~ frames^3) first, so
+  // the last wave holds the cheapest ones
+  std::vector<int> order(n_vols);
+  for (int v = 0; v < n_vols; ++v) order[v] = v;
+  if (tn.order_by_cost)
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return vols[a].geometry.cols > vols[b].geometry.cols; });
+  // the table: error word and patch work first (offset 0 of the workspace), then volumes and lists
+  const size_t tbl = batch_table_bytes(n_vols, total);
+  if (!d_ws || ws_bytes < tbl + work_bytes(1, n_max, cplx))
+    return fail(PD_ERR_WORKSPACE, "workspace too small (%zu < %zu)", ws_bytes, tbl + work_bytes(1, n_max, cplx));
+  const size_t room = ws_bytes - tbl;
+  int64_t chunk = std::max<int64_t>(1, (int64_t)(room / per_patch_bytes(n_max, cplx)));
+  if (tn.chunk_patches > 0) chunk = std::min(chunk, tn.chunk_patches);
+  chunk = std::min(chunk, total);
+  while (chunk > 1 && work_bytes((int)chunk, n_max, cplx) > room) --chunk;
+  size_t used;
+  carve_work(d_ws, (int)chunk, n_max, cplx, &used);
+  char* tb = (char*)d_ws + used;
+  VolDesc* d_vols = (VolDesc*)tb;
+  int32_t* d_list = (int32_t*)(tb + align256(sizeof(VolDesc) * n_vols));
+  int32_t* d_volof = d_list + align256(sizeof(int32_t) * total) / sizeof(int32_t);
+  static thread_local BatchTable t;  // 16 KB: a kernel parameter, built on the host
+  int64_t first = 0;
+  for (int k = 0; k < n_vols; ++k) {
+    const pd_volume& vv = vols[order[k]];
+    VolDesc& d = t.v[k].d;
+    d.g = to_geo(vv.geometry);
+    d.in = vv.d_in;
+    d.noise_std = vv.d_noise_std;
+    d.out = vv.d_out_acc;
+    d.wacc = vv.d_weight_acc;
+    d.nacc = vv.d_noise_acc;
+    d.nctr = vv.d_noise_ctr;
+    d.rank_map = vv.d_rank_map;
+    d.prank = vv.d_patch_rank;
+    d.pnoise = vv.d_patch_noise;
+    d.threshold = vv.threshold;
+    d.mp_median = vv.mp_median;
+    d.first = first;
+    t.v[k].list = vv.d_patch_list;
+    t.v[k].count = vv.n_selected;
+    first += vv.n_selected;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  PD_TRY(cuda_check(cudaMemsetAsync(d_ws, 0, sizeof(int), s), "clear error word"));
+  launch_batch_setup(t, n_vols, total, d_vols, d_list, d_volof, s);
+  // the launch shapes follow the largest patch of the batch; each CTA reads its own
+  Geo G{};
+  G.rows = m_max;
+  G.cols = n_max;
+  EigParams ep{};
+  ep.method = p->method;
+  ep.loss = p->loss;
+  ep.has_prior = p->has_prior;
+  ep.rows = m_max;
+  ep.cols = n_max;
+  ep.threshold_scale = p->threshold_scale;
+  for (int64_t off = 0; off < total; off += chunk) {
+    const int cnt = (int)std::min<int64_t>(chunk, total - off);
+    PatchWork w = carve_work(d_ws, cnt, n_max, cplx, &used);
+    w.list = d_list + off;
+    w.vols = d_vols;
+    w.vol_of = d_volof + off;
+    launch_patch_mean(G, cplx, nullptr, w, s);
+    if (p->method == PD_METHOD_HYBRID || (p->method == PD_METHOD_OPTIMAL && p->has_prior))
+      launch_prior(G, p->method, nullptr, w, s);
+    launch_gram_fp32(G, cplx, nullptr, w, s);
+    PD_TRY(cuda_check(launch_eig(cplx, n_max, ep, w, s), "eigensolver launch"));
+    SynthArgs sa{};
+    sa.recombination = p->recombination;
+    sa.list_offset = off;
+    sa.row_blocks = tn.synth_row_blocks;
+    launch_synth(G, cplx, nullptr, w, sa, s);
+    PD_TRY(cuda_check(cudaGetLastError(), "pd_denoise_batch launch"));
+  }
+  return PD_OK;
 }
 
 // ---------------------------------------------------------------------------

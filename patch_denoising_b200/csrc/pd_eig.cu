@@ -792,9 +792,23 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
                                                        pd_adaptive ad) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ __align__(16) unsigned char sm[];
+  const int p = blockIdx.x;
+  if (w.vols) {
+    // batched call: this patch's volume sets the frames and the rule's
+    // parameters; the packed matrix goes to shared memory when it fits the
+    // launch's allocation (sized for the batch's largest patch)
+    const VolDesc& v = w.vols[w.vol_of[p]];
+    n = v.g.cols;
+    ep.rows = v.g.rows;
+    ep.cols = n;
+    ep.threshold = v.threshold;
+    ep.mp_median = v.mp_median;
+    uint32_t dyn;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    in_smem = eig_layout(CPLX, n, true).total <= dyn ? 1 : 0;
+  }
   const EigLayout L = eig_layout(CPLX, n, (in_smem & 1) != 0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int p = blockIdx.x;
   if (ep.only_unfinished && w.n_active[p] >= 0) return;  // solved by k_sub
   T* G = reinterpret_cast<T*>(w.gram + (int64_t)p * w.gram_stride);
   T* A = (in_smem & 1) ? reinterpret_cast<T*>(sm + L.a) : G;
@@ -1229,7 +1243,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
       }
     }
   }
-  for (int a = tid; a < act; a += EIG_THREADS) w.coef[(int64_t)p * n + a] = acoef[a];
+  for (int a = tid; a < act; a += EIG_THREADS) w.coef[(int64_t)p * w.n_stride + a] = acoef[a];
   if (tid == 0) w.n_active[p] = act;
 }
 

@@ -17,18 +17,23 @@ constexpr int GK = 16;   // rows per k step
 constexpr int GRAM_THREADS = 256;
 
 template <bool CPLX>
-__global__ void __launch_bounds__(MEAN_THREADS) k_patch_mean(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
+__global__ void __launch_bounds__(MEAN_THREADS) k_patch_mean(Geo g, const typename Elem<CPLX>::T* in,
                                                              PatchWork w) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ int64_t rowbase[];
   const int p = blockIdx.x;
+  if (w.vols) {  // batched call: this patch's volume
+    const VolDesc& v = w.vols[w.vol_of[p]];
+    g = v.g;
+    in = reinterpret_cast<const T*>(v.in);
+  }
   const int64_t idx = w.list[p];
   int64_t o[4];
   patch_origin(g, idx, o);
   const int M = g.rows, n = g.cols;
   for (int r = threadIdx.x; r < M; r += blockDim.x) rowbase[r] = row_voxel(g, o, r) * g.shape[3] + o[3];
   __syncthreads();
-  T* mean = reinterpret_cast<T*>(w.mean) + (int64_t)p * n;
+  T* mean = reinterpret_cast<T*>(w.mean) + (int64_t)p * w.n_stride;
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
     double sx = 0.0, sy = 0.0;
     for (int r = 0; r < M; ++r) {
@@ -56,11 +61,16 @@ __global__ void __launch_bounds__(MEAN_THREADS) k_patch_mean(Geo g, const typena
 // adaptive: mean(noise_std^2), whose root is the patch's stdest.
 // (space_time/lowrank.py:106, :389 and :617; the maps are constant along time so
 // the 4D patch mean equals the spatial one.)
-__global__ void k_prior(Geo g, int method, const double* __restrict__ ns, PatchWork w) {
+__global__ void k_prior(Geo g, int method, const double* ns, PatchWork w) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int p = warp; p < w.count; p += nwarps) {
+    if (w.vols) {  // batched call: this patch's volume
+      const VolDesc& v = w.vols[w.vol_of[p]];
+      g = v.g;
+      ns = v.noise_std;
+    }
     int64_t o[4];
     patch_origin(g, w.list[p], o);
     double s = 0.0;
@@ -85,7 +95,7 @@ __device__ __forceinline__ void tile_pair(int t, int& bi, int& bj) {
 // Register-tiled 64x64 block of C = Xc^H Xc for one patch (grid.x = patch,
 // grid.y = lower tile pair).
 template <bool CPLX>
-__global__ void __launch_bounds__(GRAM_THREADS) k_gram_fp32(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
+__global__ void __launch_bounds__(GRAM_THREADS) k_gram_fp32(Geo g, const typename Elem<CPLX>::T* in,
                                                             PatchWork w) {
   using T = typename Elem<CPLX>::T;
   __shared__ T As[GK][GT];
@@ -93,12 +103,18 @@ __global__ void __launch_bounds__(GRAM_THREADS) k_gram_fp32(Geo g, const typenam
   __shared__ T mA[GT], mB[GT];
   __shared__ int64_t rb[GK];
   const int p = blockIdx.x;
+  if (w.vols) {  // batched call: this patch's volume
+    const VolDesc& v = w.vols[w.vol_of[p]];
+    g = v.g;
+    in = reinterpret_cast<const T*>(v.in);
+  }
   int bi, bj;
   tile_pair(blockIdx.y, bi, bj);
   const int n = g.cols, M = g.rows;
+  if (bi * GT >= n) return;  // a tile of a larger patch of the batch
   int64_t o[4];
   patch_origin(g, w.list[p], o);
-  const T* mean = reinterpret_cast<const T*>(w.mean) + (int64_t)p * n;
+  const T* mean = reinterpret_cast<const T*>(w.mean) + (int64_t)p * w.n_stride;
   const int tid = threadIdx.x;
   if (tid < GT) {
     const int ca = bi * GT + tid, cb = bj * GT + tid;

@@ -25,8 +25,39 @@ __global__ void k_compact(const uint8_t* flags, int64_t n, const int32_t* boff, 
 // Gram timed out; PD_DEVERR_NONFINITE a processed patch holds a NaN or inf sample.
 constexpr int PD_DEVERR_NONFINITE = 7;
 
+// One volume of a batched call (pd_denoise_batch): its geometry, buffers and
+// per-volume decision parameters, read by the patch kernels through vol_of.
+struct VolDesc {
+  Geo g;
+  const void* in;
+  const double* noise_std;
+  void* out;
+  float* wacc;
+  float* nacc;
+  float* nctr;
+  int32_t* rank_map;
+  int32_t* prank;   // per listed patch of this volume
+  float* pnoise;
+  double threshold;  // raw
+  double mp_median;  // optimal
+  int64_t first;     // work-list position of the volume's first patch
+};
+
+// Host-built table of a batched call, passed by value to k_batch_setup (the
+// volumes are in work-list order: volume v's patches start at d.first).
+struct BatchVolume {
+  VolDesc d;
+  const int32_t* list;  // the volume's selected patches
+  int64_t count;
+};
+struct BatchTable {
+  BatchVolume v[PD_BATCH_MAX_VOLUMES];
+};
+void launch_batch_setup(const BatchTable& t, int nv, int64_t total, VolDesc* vols, int32_t* list, int32_t* vol_of,
+                        cudaStream_t s);
+
 struct PatchWork {
-  const int32_t* list;  // linear patch indices of the chunk
+  const int32_t* list;  // linear patch indices of the chunk (within their volume)
   int32_t count;        // patches in the chunk
   float* mean;          // [count][n] (complex: 2n floats)
   float* gram;          // [count][gram_stride] packed lower Gram
@@ -40,6 +71,9 @@ struct PatchWork {
   double* prior;        // [count] hybrid varest / optimal sigma prior
   int* err;             // device error word (0 = ok)
   void* packed;         // mixed precision: bf16 hi/lo operands of the chunk
+  int32_t n_stride;     // frames per patch slot of mean / coef (the largest n of a batch)
+  const VolDesc* vols;  // batched call: the volumes (NULL: one volume, the launch's Geo)
+  const int32_t* vol_of;  // batched call: volume of each chunk patch
 };
 
 // pd_gram.cu
@@ -84,6 +118,7 @@ struct SynthArgs {
   float* patch_noise;
   int64_t list_offset;  // position of the chunk inside the full list
   int wide;             // high ranks expected (adaptive shrinkage): the grouped-reduction kernel
+  int row_blocks;       // CTAs per patch (0: by the patch's rows, at most 8)
 };
 void launch_synth(const Geo& g, bool cplx, const void* in, const PatchWork& w, const SynthArgs& a,
                   cudaStream_t s);

@@ -26,20 +26,32 @@ __device__ __forceinline__ void acc_add(cf* p, cf v) {
 // WIDE: with the grouped reduction for ranks above 8 (adaptive launches only;
 // its registers would cost the low-rank methods occupancy).
 template <bool CPLX, int NS, int R, bool WIDE>
-__global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
+__global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Elem<CPLX>::T* in,
                                                        PatchWork w, SynthArgs sa, int ysplit) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ __align__(16) unsigned char sm[];
-  const int n = g.cols, M = g.rows;
-  T* ys = reinterpret_cast<T*>(sm);  // [SYN_NW][R][n]
-  T* smean = ys + SYN_NW * R * n;    // [n]
-  float* scoef = reinterpret_cast<float*>(smean + n);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   // grid: patches x ysplit row blocks, flattened patch-major (the blocks of a
   // patch, and of its overlapping neighbours, read and scatter to the same
   // voxels close together in time)
   const int p = (int)(blockIdx.x / (unsigned)ysplit);
   const int yb = (int)(blockIdx.x - (unsigned)p * (unsigned)ysplit);
+  if (w.vols) {  // batched call: this patch's volume and its output buffers
+    const VolDesc& v = w.vols[w.vol_of[p]];
+    g = v.g;
+    in = reinterpret_cast<const T*>(v.in);
+    sa.out = v.out;
+    sa.weight_acc = v.wacc;
+    sa.noise_acc = v.nacc;
+    sa.noise_ctr = v.nctr;
+    sa.rank_map = v.rank_map;
+    sa.patch_rank = v.prank - v.first;  // records at the volume's own list positions
+    sa.patch_noise = v.pnoise - v.first;
+  }
+  const int n = g.cols, M = g.rows;
+  T* ys = reinterpret_cast<T*>(sm);  // [SYN_NW][R][n]
+  T* smean = ys + SYN_NW * R * n;    // [n]
+  float* scoef = reinterpret_cast<float*>(smean + n);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t pidx = w.list[p];
   int64_t o[4];
   patch_origin(g, pidx, o);
@@ -47,9 +59,9 @@ __global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Ele
   const int act = w.n_active[p];
   const int rank = w.rank[p];
   const float nv = w.noise[p];
-  const T* mean = reinterpret_cast<const T*>(w.mean) + (int64_t)p * n;
+  const T* mean = reinterpret_cast<const T*>(w.mean) + (int64_t)p * w.n_stride;
   for (int t = tid; t < n; t += SYN_THREADS) smean[t] = mean[t];
-  for (int a = tid; a < act; a += SYN_THREADS) scoef[a] = w.coef[(int64_t)p * n + a];
+  for (int a = tid; a < act; a += SYN_THREADS) scoef[a] = w.coef[(int64_t)p * w.n_stride + a];
   const float* vb = w.vec + (int64_t)p * w.vec_stride;
   const int n2 = 2 * n;
   const int64_t T4 = g.shape[3];
@@ -212,6 +224,7 @@ static void synth_ns(const Geo& g, const void* in, const PatchWork& w, const Syn
   const int rows_per_block = SYN_NW * R;
   int ysplit = (g.rows + rows_per_block - 1) / rows_per_block;
   if (ysplit > 8) ysplit = 8;
+  if (a.row_blocks > 0) ysplit = a.row_blocks;  // a tuned split
   if (a.recombination == PD_RECOMB_CENTER) ysplit = 1;
   const unsigned grid = (unsigned)((int64_t)w.count * ysplit);
   PD_TIMED("synth_scatter", s, kern<<<grid, SYN_THREADS, smem, s>>>(g, (const T*)in, w, a, ysplit));

@@ -209,7 +209,7 @@ def test_adaptive_argument_errors_match_the_reference():
 
 
 def test_ctypes_structs_match_the_c_header(tmp_path):
-    """pd_geometry, pd_params and pd_adaptive: the ctypes mirrors have the C layout
+    """pd_geometry, pd_params, pd_adaptive, pd_volume and pd_batch_tuning: the ctypes mirrors have the C layout
     (size and every field offset), checked by compiling the header with the C compiler."""
     import shutil
     import subprocess
@@ -217,7 +217,8 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no C compiler")
-    structs = {"pd_geometry": _lib.Geometry, "pd_params": _lib.Params, "pd_adaptive": _lib.Adaptive}
+    structs = {"pd_geometry": _lib.Geometry, "pd_params": _lib.Params, "pd_adaptive": _lib.Adaptive,
+               "pd_volume": _lib.Volume, "pd_batch_tuning": _lib.BatchTuning}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "patch_denoise_b200.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
