@@ -250,6 +250,102 @@ def roofline(name, per_launch_ms, launches, steps, work, kind, peaks):
             "per_launch_ms": per_launch_ms, "launches": launches}
 
 
+def _event_ms(fn, reps=1):
+    """Device time of ``fn()`` (CUDA events on the current stream), best of ``reps``."""
+    import torch
+
+    best = float("inf")
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        best = min(best, a.elapsed_time(b))
+    return best
+
+
+def run_extras(dev, dist):
+    """The other configurations, each timed on this GPU (synthetic inputs of the
+    configurations' shapes, generated on the device):
+    config 3, 16 uneven volumes in one batched call vs per-volume calls;
+    config 4, the differentiable layer's forward and backward at full size;
+    config 5, hybrid-PCA on the 1.6 GB volume (mixed and plain FP32)."""
+    import torch
+
+    from patch_denoising_b200 import HybridPCADenoiser, OptimalSVDDenoiser
+    from patch_denoising_b200.batch import denoise_batch
+    from patch_denoising_b200.space_time import lowrank_denoise
+    from patch_denoising_b200.synthetic import ellipsoid_mask, lowrank_volume_torch, radial_noise_map
+
+    out = {}
+    # ---- config 3: 16 volumes, sizes U[48..96] x U[48..96] x U[32..60] x U[100..343], rank 3-10,
+    # sigma U[2, 8], ellipsoid masks ~55 %, optimal fro, patch 7 overlap 4
+    rng = np.random.default_rng(3)
+    vols, masks, vf = [], [], 0.0
+    for i in range(16):
+        sh = (int(rng.integers(48, 97)), int(rng.integers(48, 97)), int(rng.integers(32, 61)),
+              int(rng.integers(100, 344)))
+        vols.append(lowrank_volume_torch(sh, int(rng.integers(3, 11)), noise=float(rng.uniform(2, 8)), seed=100 + i,
+                                         device=dev))
+        masks.append(ellipsoid_mask(sh[:-1], fill=0.55, seed=i))
+        vf += float(np.prod(sh))
+    res, tn = denoise_batch(vols, "optimal", 7, 4, "weighted", masks, 50, return_tuning=True)
+    del res
+    t_batch = _event_ms(lambda: denoise_batch(vols, "optimal", 7, 4, "weighted", masks, 50, tuning=tn), reps=2)
+
+    def per_volume():
+        for x, m in zip(vols, masks):
+            OptimalSVDDenoiser(7, 4, loss="fro").denoise(x, mask=m, mask_threshold=50)
+
+    t_single = _event_ms(per_volume, reps=2)
+    out["batched_config3"] = {
+        "workload": "16 float32 volumes U[48..96]x[48..96]x[32..60]x[100..343], rank 3-10, sigma U[2,8], "
+                    "ellipsoid masks ~55%, optimal fro, patch 7 overlap 4 (T <= 343: the reference's MP median "
+                    "needs T <= M)",
+        "voxel_frames": vf, "batched_ms": t_batch, "per_volume_ms": t_single,
+        "batched_value": vf / (t_batch * 1e-3), "per_volume_value": vf / (t_single * 1e-3),
+        "unit": "voxel-frames/s", "tuning": tn}
+    del vols
+    torch.cuda.empty_cache()
+    # ---- config 4: differentiable MP-PCA/SVT layer, 64x64x40x120, N(0, 4^2), patch 7 overlap 6 (stride 1)
+    x = lowrank_volume_torch((64, 64, 40, 120), 5, noise=4.0, seed=4, device=dev).requires_grad_(True)
+    scale = torch.tensor(1.0, device=dev, requires_grad=True)
+    y = lowrank_denoise(x, 7, 6, scale, 4.0)
+    torch.cuda.synchronize()
+    holder = {}
+    t_fwd = _event_ms(lambda: holder.__setitem__("y", lowrank_denoise(x, 7, 6, scale, 4.0)))
+    g = torch.where(torch.isfinite(holder["y"]), torch.ones_like(holder["y"]), torch.zeros_like(holder["y"]))
+    t_bwd = _event_ms(lambda: holder["y"].backward(g, retain_graph=True))
+    vf4 = float(64 * 64 * 40 * 120)
+    out["differentiable_config4"] = {
+        "workload": "soft-threshold layer, float32 64x64x40x120, rank 5 + N(0,4^2), patch 7 overlap 6 "
+                    "(114376 patches), learnable threshold_scale; backward w.r.t. input and threshold_scale",
+        "forward_ms": t_fwd, "backward_ms": t_bwd, "forward_value": vf4 / (t_fwd * 1e-3),
+        "backward_value": vf4 / (t_bwd * 1e-3), "unit": "voxel-frames/s",
+        "threshold_grad": float(scale.grad) if scale.grad is not None else None}
+    del x, y, holder, g
+    torch.cuda.empty_cache()
+    # ---- config 5: hybrid-PCA, 128x128x80x300 (1.57 GB), rank 8, sigma(x) = 3 + 2 r / r_max, patch 11 overlap 8
+    nmap = radial_noise_map((128, 128, 80))
+    x5 = lowrank_volume_torch((128, 128, 80, 300), 8, noise=1.0, noise_map=nmap, seed=5, device=dev)
+    vf5 = float(x5.numel())
+    c5 = {"workload": "hybrid-PCA float32 128x128x80x300, rank 8, sigma(x) = 3 + 2 r/r_max as the noise map, "
+                      "patch 11 overlap 8 (38400 patches)", "unit": "voxel-frames/s"}
+    for prec in ("mixed", "fp32"):
+        den = HybridPCADenoiser(11, 8, precision=prec)
+        res = den.denoise(x5, noise_std=nmap)
+        c5[f"{prec}_finite_fraction"] = float(torch.isfinite(res[0]).float().mean())
+        del res
+        ms = _event_ms(lambda: HybridPCADenoiser(11, 8, precision=prec).denoise(x5, noise_std=nmap))  # noqa: B023
+        c5[f"{prec}_ms"] = ms
+        c5[f"{prec}_value"] = vf5 / (ms * 1e-3)
+    out["hybrid_config5"] = c5
+    del x5
+    torch.cuda.empty_cache()
+    return out
+
+
 def max_over_ranks(value, dist, device):
     """The largest per-rank value (the job's time), or ``value`` itself on one rank."""
     if dist is None:
@@ -382,6 +478,8 @@ def ours_arm(args, rank, world):
     h2d = x.nbytes
     d2h = out.nbytes + w.nbytes + nm.nbytes + rm.nbytes
 
+    extras = run_extras(dev, dist) if not args.no_extras else {}
+
     if rank == 0:
         launches = int(sum(v[0] for v in kern.values())) // max(args.steps, 1)
         top = max(kern.items(), key=lambda kv: kv[1][1]) if kern else None
@@ -422,6 +520,7 @@ def ours_arm(args, rank, world):
             "kernels_ms_per_step": {k: v[1] / args.steps for k, v in kern.items()},
             "gpu_launches": launches,
             "clocks": clocks,
+            **extras,
         }
         if world == 1 and not args.no_cpu:
             t_cpu = cpu_full_call(x)
@@ -442,7 +541,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "mixed"], default="mixed")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline call")
+    ap.add_argument("--no-extras", action="store_true", help="skip the other configurations' timings")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

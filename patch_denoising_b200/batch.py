@@ -202,7 +202,7 @@ def denoise_batch(volumes, method, patch_shape, patch_overlap, recombination="we
         elif tuning is None:
             tn = dict(synth_row_blocks=0, order_by_cost=1, chunk_patches=0)
         else:
-            tn = dict(synth_row_blocks=0, order_by_cost=1, chunk_patches=0, **tuning)
+            tn = {**dict(synth_row_blocks=0, order_by_cost=1, chunk_patches=0), **tuning}
         prep.run(tn)
         res = [r[:4] for r in prep.finalize()]
     return (res, tn) if return_tuning else res

@@ -435,9 +435,9 @@ pd_status pd_nordic_workspace_size(int64_t rows, int64_t cols, int32_t n_iter, s
   if (rows < 1 || cols < 1 || n_iter < 1) return fail(PD_ERR_INVALID, "empty Monte-Carlo problem");
   if (cols > MAX_FRAMES) return fail(PD_ERR_UNSUPPORTED, "at most %d frames", MAX_FRAMES);
   const size_t simt = align256(sizeof(float) * (size_t)n_iter * mc_chunks(rows) * pk_size((int)cols));
-  const size_t tc = align256(gauss_packed_bytes(rows, (int)cols, n_iter)) +
-                    align256(sizeof(float) * (size_t)n_iter * gauss_chunks(rows, (int)cols) * pk_size((int)cols));
-  *bytes = work_bytes(n_iter, (int)cols, false) + std::max(simt, tc);
+  const int64_t d = std::min(rows, cols);
+  const size_t wish = align256(sizeof(float) * (size_t)n_iter * d * d);
+  *bytes = work_bytes(n_iter, (int)cols, false) + std::max(simt, wish);
   return PD_OK;
 }
 
@@ -453,23 +453,23 @@ static pd_status mc_launch(int64_t rows, int64_t cols, int32_t n_iter, uint64_t 
   size_t used;
   PatchWork w = carve_work(d_ws, n_iter, n, false, &used);
   PD_TRY(cuda_check(cudaMemsetAsync(w.err, 0, sizeof(int), s), "clear error word"));
+  int ne = n;  // order of the Grams whose top eigenvalue is taken
   if (precision == PD_PRECISION_MIXED) {
-    // generate the draws packed as bf16 G^T, TMA-fed tensor-core Gram over K chunks, ordered reduction
-    void* packed = (char*)d_ws + used;
-    float* part = (float*)((char*)packed + align256(gauss_packed_bytes(rows, n, n_iter)));
-    const int chunks = (int)gauss_chunks(rows, n);
-    PD_TRY(cuda_check(launch_gauss_gram_packed(rows, n, n_iter, seed, packed, part, pk_size(n), w.err, s),
-                      "Monte-Carlo Gram"));
-    launch_chunk_reduce(part, pk_size(n), chunks, pk_size(n), n_iter, w.gram, w.gram_stride, s);
+    // the chosen path: each draw's Gram sampled directly from its Wishart law
+    // (Bartlett), of order min(rows, cols) (G G^T and G^T G share their top eigenvalue)
+    ne = (int)std::min<int64_t>(rows, n);
+    launch_wishart(std::max<int64_t>(rows, n), ne, n_iter, seed, (float*)((char*)d_ws + used), w.gram,
+                   w.gram_stride, s);
   } else {
+    // plain FP32: the explicit rows x cols Gaussian draws and their Grams, as the reference
     float* part = (float*)((char*)d_ws + used);
     launch_mc_gram(rows, n, n_iter, seed, part, w.gram, w.gram_stride, s);
   }
   EigParams ep{};
   ep.method = EIG_MODE_TOP1;
   ep.rows = (int)std::min<int64_t>(rows, INT32_MAX);
-  ep.cols = n;
-  PD_TRY(cuda_check(launch_eig(false, n, ep, w, s), "Monte-Carlo eigensolver launch"));
+  ep.cols = ne;
+  PD_TRY(cuda_check(launch_eig(false, ne, ep, w, s), "Monte-Carlo eigensolver launch"));
   *out = w;
   return PD_OK;
 }

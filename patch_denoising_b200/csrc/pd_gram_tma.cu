@@ -6,13 +6,11 @@
 //   rounded up to 64, zero padded), x = hi + lo to about 16 bits. Reads are
 //   coalesced along frames, writes along voxels through a shared-memory
 //   transpose; the kernel is memory bound and runs at full occupancy.
-// k_gauss_pack: the same layout for the NORDIC Monte-Carlo draws (bf16 hi only),
-//   generating the normals of (seed, draw, row, column) directly.
-// k_gram_tma: CTA = (patch or row chunk, 128 x <=256 block of the lower Gram).
+// k_gram_tma: CTA = (patch, 128 x <=256 block of the lower Gram).
 //   One thread issues cp.async.bulk.tensor loads (128-byte swizzle, the
 //   canonical K-major layout of tcgen05) into a 2-stage ring guarded by
 //   mbarriers with transaction counts; one thread issues tcgen05.mma with the
-//   accumulator in TMEM (hi*hi + hi*lo + lo*hi, or hi*hi for the draws);
+//   accumulator in TMEM (hi*hi + hi*lo + lo*hi);
 //   four warps read TMEM and write the packed Gram (complex via 2x2 blocks).
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -124,28 +122,6 @@ __global__ void __launch_bounds__(256) k_pack_patches(Geo g, const float* __rest
   }
 }
 
-// Gaussian draws, packed transposed: G^T[d][c][r] for r < rows (zero to kp).
-// A thread makes the normals of two consecutive rows and one group of four
-// columns (two Philox blocks) and stores them as bf16 pairs straight into the
-// four K-major column rows: a warp covers 64 consecutive rows, so every store
-// instruction writes 128 contiguous bytes, with no shared-memory transpose.
-// grid: (kp / 64, ceil(cols / 32), draws), 256 threads = 8 column groups.
-__global__ void __launch_bounds__(256) k_gauss_pack(int64_t rows, int cols, uint64_t seed,
-                                                    __nv_bfloat16* __restrict__ out, int64_t kp) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t r = (int64_t)blockIdx.x * PK_R + 2 * lane;
-  const int cg = blockIdx.y * 8 + warp;  // columns 4 cg .. 4 cg + 3
-  const int d = blockIdx.z;
-  if (4 * cg >= cols) return;
-  float z0[4] = {0.f, 0.f, 0.f, 0.f}, z1[4] = {0.f, 0.f, 0.f, 0.f};
-  if (r < rows) normals4(seed, (uint32_t)d, (uint64_t)r, (uint32_t)cg, z0);
-  if (r + 1 < rows) normals4(seed, (uint32_t)d, (uint64_t)(r + 1), (uint32_t)cg, z1);
-  __nv_bfloat16* op = out + ((int64_t)d * cols + 4 * cg) * kp + r;
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-    if (4 * cg + q < cols) *reinterpret_cast<__nv_bfloat162*>(op + (int64_t)q * kp) = __floats2bfloat162_rn(z0[q], z1[q]);
-}
-
 // ---------------------------------------------------------------------------
 // TMA + tcgen05 Gram
 // ---------------------------------------------------------------------------
@@ -155,10 +131,7 @@ struct TmaArgs {
   int cplx;
   int split;   // 3: hi/lo, 1: hi only
   int64_t kp;  // packed K extent
-  int dense;   // 1: Grams of K chunks of dense draws (one partial per draw and chunk)
-  int64_t k_per_cta;
-  int nblk;    // Gram blocks per patch or per K chunk (grid flattened with the block fastest)
-  int chunks;  // dense: K chunks per draw
+  int nblk;    // Gram blocks per patch (grid flattened with the block fastest)
   float* out;
   int64_t out_stride;
   int* err;
@@ -202,9 +175,8 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
   uint64_t* done = bars + 2 * TM_STAGES;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
 
-  // The Gram blocks that read the same operand rows (of one patch, or of one
-  // K chunk of a draw) are consecutive in the flattened grid, so they share
-  // those rows in L2: patch mode (patch, block), dense mode (draw, chunk, block).
+  // The Gram blocks that read the same operand rows (of one patch) are
+  // consecutive in the flattened grid (patch, block), so they share those rows in L2.
   const int bidx = (int)(blockIdx.x % (unsigned)a.nblk);
   const int pidx = (int)(blockIdx.x / (unsigned)a.nblk);
   int rb, nb, ncols;
@@ -214,18 +186,9 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
   uint32_t tcols = 32;
   while (tcols < (uint32_t)npad) tcols <<= 1;
 
-  int64_t k_begin = 0, k_end = a.kp;
-  int zc = pidx;  // third tensor-map coordinate: patch, or draw
-  float* out;
-  if (a.dense) {
-    const int chunk = pidx % a.chunks;  // pidx = draw * chunks + chunk
-    k_begin = (int64_t)chunk * a.k_per_cta;
-    k_end = min(k_begin + a.k_per_cta, a.kp);
-    zc = pidx / a.chunks;
-    out = a.out + (int64_t)pidx * a.out_stride;
-  } else {
-    out = a.out + (int64_t)pidx * a.out_stride;
-  }
+  const int64_t k_begin = 0, k_end = a.kp;
+  const int zc = pidx;  // third tensor-map coordinate: the patch
+  float* out = a.out + (int64_t)pidx * a.out_stride;
   const int nch = (int)((k_end - k_begin + 63) / 64);
   const uint32_t tx_bytes = (split ? 2u : 1u) * (TM_TILE_A + (uint32_t)nbox * TM_BOX * 128u);
 
@@ -414,7 +377,6 @@ cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const Pa
   a.cplx = cplx ? 1 : 0;
   a.split = 3;
   a.kp = kp;
-  a.dense = 0;
   a.nblk = tm_blocks(N);
   a.out = w.gram;
   a.out_stride = w.gram_stride;
@@ -425,52 +387,6 @@ cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const Pa
   const unsigned grid = (unsigned)(w.count * a.nblk);
   PD_TIMED("gram_tc", s, k_gram_tma<<<grid, TM_THREADS, smem, s>>>(mh, ml, a));
   return cudaGetLastError();
-}
-
-size_t gauss_packed_bytes(int64_t rows, int cols, int n_iter) { return (size_t)2 * cols * pack_k(rows) * n_iter; }
-
-int64_t gauss_k_per_cta(int64_t rows, int cols) {
-  // about 2 waves of CTAs over the draws' row chunks
-  const int blocks = tm_blocks(cols);
-  int64_t chunks = (2 * 148 + blocks - 1) / blocks;
-  int64_t k = (pack_k(rows) + chunks - 1) / chunks;
-  return (k + 63) & ~int64_t(63);
-}
-
-cudaError_t launch_gauss_gram_packed(int64_t rows, int cols, int n_iter, uint64_t seed, void* packed, float* part,
-                                     int64_t part_stride, int* err, cudaStream_t s) {
-  const int64_t kp = pack_k(rows);
-  __nv_bfloat16* g = reinterpret_cast<__nv_bfloat16*>(packed);
-  dim3 pg((unsigned)(kp / PK_R), (cols + 31) / 32, n_iter);
-  PD_TIMED("gauss_pack", s, k_gauss_pack<<<pg, 256, 0, s>>>(rows, cols, seed, g, kp));
-  CUtensorMap mh;
-  cudaError_t e = make_map(&mh, g, kp, cols, n_iter);
-  if (e != cudaSuccess) return e;
-  TmaArgs a{};
-  a.N = cols;
-  a.n_out = cols;
-  a.split = 1;
-  a.kp = kp;
-  a.dense = 1;
-  a.k_per_cta = gauss_k_per_cta(rows, cols);
-  a.out = part;
-  a.out_stride = part_stride;
-  a.err = err;
-  const size_t smem = tm_smem(1);
-  e = cudaFuncSetAttribute(k_gram_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const int64_t chunks = (kp + a.k_per_cta - 1) / a.k_per_cta;
-  a.chunks = (int)chunks;
-  a.nblk = tm_blocks(cols);
-  if ((int64_t)n_iter * chunks * a.nblk > INT32_MAX) return cudaErrorInvalidConfiguration;
-  const unsigned grid = (unsigned)((int64_t)n_iter * chunks * a.nblk);
-  PD_TIMED("mc_gram_tc", s, k_gram_tma<<<grid, TM_THREADS, smem, s>>>(mh, mh, a));
-  return cudaGetLastError();
-}
-
-int64_t gauss_chunks(int64_t rows, int cols) {
-  const int64_t k = gauss_k_per_cta(rows, cols);
-  return (pack_k(rows) + k - 1) / k;
 }
 
 }  // namespace pd

@@ -148,15 +148,13 @@ cudaError_t launch_backward(const Geo& g, const float* in, const float* gout, co
 size_t packed_bytes_per_patch(int n, bool cplx, int M);
 cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const PatchWork& w, void* packed,
                                cudaStream_t s);
-size_t gauss_packed_bytes(int64_t rows, int cols, int n_iter);
-int64_t gauss_chunks(int64_t rows, int cols);
-cudaError_t launch_gauss_gram_packed(int64_t rows, int cols, int n_iter, uint64_t seed, void* packed, float* part,
-                                     int64_t part_stride, int* err, cudaStream_t s);
 
 // pd_mc.cu
+// Bartlett-sampled Wishart Grams: n_iter packed d x d Grams distributed as G^T G
+// for m x d standard Gaussian G (m >= d); Lbuf holds n_iter d x d floats.
+void launch_wishart(int64_t m, int d, int n_iter, uint64_t seed, float* Lbuf, float* gram, int64_t gram_stride,
+                    cudaStream_t s);
 int64_t mc_chunks(int64_t rows);
-void launch_chunk_reduce(const float* part, int64_t part_stride, int chunks, int64_t np, int draws, float* gram,
-                         int64_t gram_stride, cudaStream_t s);
 // pd_noise.cu
 void launch_estimate_noise(const float* in, bool cplx, const int64_t dims[3], const int blk[3], int T, double* mean,
                            double* m2, double* out, cudaStream_t s);

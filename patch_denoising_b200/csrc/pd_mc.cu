@@ -100,11 +100,6 @@ __global__ void k_mc_reduce(const float* __restrict__ part, int64_t part_stride,
 
 int64_t mc_chunks(int64_t rows) { return (rows + MC_ROWS_PER_CTA - 1) / MC_ROWS_PER_CTA; }
 
-void launch_chunk_reduce(const float* part, int64_t part_stride, int chunks, int64_t np, int draws, float* gram,
-                         int64_t gram_stride, cudaStream_t s) {
-  dim3 rgrid((unsigned)((np + 255) / 256), draws);
-  PD_TIMED("mc_reduce", s, k_mc_reduce<<<rgrid, 256, 0, s>>>(part, part_stride, chunks, np, gram, gram_stride));
-}
 
 // level = mean_i sqrt(max(lam_i, 0)) in draw order (the host formula of
 // pd_nordic_mc_threshold, so both give the same double); out = {level, noise_std * level}.
@@ -131,6 +126,92 @@ void launch_mc_gram(int64_t rows, int cols, int n_iter, uint64_t seed, float* pa
   PD_TIMED("mc_gram", s, k_mc_gram<<<grid, MC_THREADS, 0, s>>>(rows, cols, seed, part, np));
   dim3 rgrid((unsigned)((np + 255) / 256), n_iter);
   PD_TIMED("mc_reduce", s, k_mc_reduce<<<rgrid, 256, 0, s>>>(part, np, (int)chunks, np, gram, gram_stride));
+}
+
+}  // namespace pd
+
+namespace pd {
+
+// ---------------------------------------------------------------------------
+// Wishart Grams by Bartlett's decomposition (M. S. Bartlett, 1933): for G an
+// m x d standard Gaussian matrix (m >= d), G^T G has the law of L L^T with L
+// lower triangular, L_ij ~ N(0, 1) for i > j and L_ii^2 ~ chi-square with
+// m - i degrees of freedom (i = 0 .. d - 1), all independent. Its largest
+// eigenvalue is then distributed as the squared largest singular value of G,
+// from d (d + 1) / 2 random numbers instead of m d.
+// ---------------------------------------------------------------------------
+
+// Gamma(a, 1) variate (Marsaglia & Tsang, ACM TOMS 2000; a < 1 through
+// Gamma(a + 1) U^(1/a)), FP64, from counter-based uniforms and normals of
+// (seed, draw, i); bounded to 64 rejection rounds (the acceptance rate exceeds
+// 95 % for every a).
+__device__ double gamma_mt(double a, uint64_t seed, uint32_t draw, uint32_t i) {
+  double boost = 1.0;
+  uint32_t ctr = 0;
+  auto words = [&](uint32_t c[4]) {
+    c[0] = ctr++;
+    c[1] = i;
+    c[2] = 0x80000000u;  // a counter space of its own (off-diagonal rows use row hi = 0)
+    c[3] = draw;
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  };
+  if (a < 1.0) {
+    uint32_t c[4];
+    words(c);
+    const double u = ((double)c[0] + 1.0) * 2.3283064365386963e-10;
+    boost = pow(u, 1.0 / a);
+    a += 1.0;
+  }
+  const double dd = a - 1.0 / 3.0, cc = 1.0 / sqrt(9.0 * dd);
+  for (int it = 0; it < 64; ++it) {
+    uint32_t c[4];
+    words(c);
+    const double u1 = ((double)c[0] + 1.0) * 2.3283064365386963e-10;
+    const double u2 = (double)c[1] * 2.3283064365386963e-10;
+    const double x = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+    double v = 1.0 + cc * x;
+    if (v <= 0.0) continue;
+    v = v * v * v;
+    const double u = ((double)c[2] + 1.0) * 2.3283064365386963e-10;
+    if (u < 1.0 - 0.0331 * x * x * x * x || log(u) < 0.5 * x * x + dd * (1.0 - v + log(v))) return dd * v * boost;
+  }
+  return dd * boost;  // not reached in practice: the mean
+}
+
+// One CTA per draw: L (d x d, row-major, lower part) into Lbuf, then the packed
+// lower W = L L^T (FP64 sums) into gram.
+__global__ void __launch_bounds__(256) k_wishart(int64_t m, int d, uint64_t seed, float* __restrict__ Lbuf,
+                                                 float* __restrict__ gram, int64_t gram_stride) {
+  const uint32_t draw = blockIdx.x;
+  float* L = Lbuf + (int64_t)draw * d * d;
+  const int ng = (d + 3) / 4;
+  for (int t = threadIdx.x; t < d * ng; t += blockDim.x) {
+    const int i = t / ng, cg = t % ng;
+    if (4 * cg >= i) continue;
+    float z[4];
+    normals4(seed, draw, (uint64_t)i, (uint32_t)cg, z);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (4 * cg + q < i) L[(int64_t)i * d + 4 * cg + q] = z[q];
+  }
+  for (int i = threadIdx.x; i < d; i += blockDim.x)
+    L[(int64_t)i * d + i] = (float)sqrt(2.0 * gamma_mt(0.5 * (double)(m - i), seed, draw, (uint32_t)i));
+  __syncthreads();
+  float* W = gram + (int64_t)draw * gram_stride;
+  for (int j = 0; j < d; ++j) {
+    const float* lj = L + (int64_t)j * d;
+    for (int i = j + threadIdx.x; i < d; i += blockDim.x) {
+      const float* li = L + (int64_t)i * d;
+      double s = 0.0;
+      for (int k = 0; k <= j; ++k) s += (double)li[k] * lj[k];
+      W[pk(i, j, d)] = (float)s;
+    }
+  }
+}
+
+void launch_wishart(int64_t m, int d, int n_iter, uint64_t seed, float* Lbuf, float* gram, int64_t gram_stride,
+                    cudaStream_t s) {
+  PD_TIMED("mc_wishart", s, k_wishart<<<n_iter, 256, 0, s>>>(m, d, seed, Lbuf, gram, gram_stride));
 }
 
 }  // namespace pd

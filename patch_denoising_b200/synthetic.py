@@ -81,3 +81,29 @@ def radial_noise_map(spatial_shape, base=3.0, extra=2.0):
     centre = [(s - 1) / 2 for s in spatial_shape]
     r = np.sqrt(sum((g - c) ** 2 for g, c in zip(grids, centre)))
     return base + extra * r / r.max()
+
+
+def lowrank_volume_torch(shape, rank, *, amplitude=100.0, sigma_space=4.0, periods=(8.0, 30.0), noise=5.0,
+                         noise_map=None, seed=0, device="cuda"):
+    """``lowrank_volume``'s construction (real), generated on the device with a
+    seeded torch generator: for volumes of gigabytes, where host generation is
+    slow. The same law, other random draws. Returns the float32 noisy volume."""
+    import torch
+
+    gen = torch.Generator(device=device).manual_seed(seed)
+    spatial = shape[:-1]
+    grids = torch.meshgrid(*[torch.arange(s, dtype=torch.float32, device=device) for s in spatial], indexing="ij")
+    t = torch.arange(shape[-1], dtype=torch.float32, device=device)
+    out = torch.zeros(shape, dtype=torch.float32, device=device)
+    for _ in range(rank):
+        u = torch.rand(len(spatial) + 2, generator=gen, device=device)
+        centre = [float(u[i]) * (s - 1) for i, s in enumerate(spatial)]
+        r2 = sum((g - c) ** 2 for g, c in zip(grids, centre))
+        blob = amplitude * torch.exp(-0.5 * r2 / sigma_space**2)
+        period = periods[0] + float(u[-2]) * (periods[1] - periods[0])
+        course = torch.sin(2 * np.pi * t / period + 2 * np.pi * float(u[-1]))
+        out += blob[..., None] * course
+    sd = torch.full(spatial, float(noise), device=device) if noise_map is None else \
+        float(noise) * torch.as_tensor(noise_map, dtype=torch.float32, device=device)
+    out += torch.randn(shape, generator=gen, device=device) * sd[..., None]
+    return out
