@@ -57,6 +57,7 @@ struct Carver {
 constexpr int MAX_FRAMES = 448;
 constexpr int MAX_ROWS = 16384;
 constexpr size_t DEFAULT_CHUNK_BUDGET = size_t(4) << 30;
+constexpr size_t BATCH_CHUNK_BUDGET = size_t(16) << 30;  // a batch spans many volumes: fewer, larger chunks
 
 int64_t gram_stride_floats(int n, bool cplx) {
   int64_t f = pk_size(n) * (cplx ? 2 : 1);
@@ -355,7 +356,7 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
   while (chunk > 1 && work_bytes((int)chunk, n, cplx, pk_b) > ws_bytes) --chunk;
   cudaStream_t s = (cudaStream_t)stream;
   const Geo G = to_geo(*g);
-  EigParams ep;
+  EigParams ep{};
   ep.method = p->method;
   ep.loss = p->loss;
   ep.has_prior = p->has_prior;
@@ -610,7 +611,7 @@ pd_status pd_denoise_batch_workspace_size(const pd_volume* vols, int32_t n_vols,
   PD_TRY(batch_check(vols, n_vols, p, &n_max, &m_max, &total));
   if (!bytes) return fail(PD_ERR_INVALID, "NULL output");
   const bool cplx = p->is_complex != 0;
-  int64_t chunk = (int64_t)std::max<size_t>(1, DEFAULT_CHUNK_BUDGET / per_patch_bytes(n_max, cplx));
+  int64_t chunk = (int64_t)std::max<size_t>(1, BATCH_CHUNK_BUDGET / per_patch_bytes(n_max, cplx));
   if (chunk_patches > 0) chunk = std::min(chunk, chunk_patches);
   chunk = std::min<int64_t>(chunk, std::max<int64_t>(total, 1));
   *bytes = work_bytes((int)chunk, n_max, cplx) + batch_table_bytes(n_vols, total);
@@ -701,11 +702,27 @@ pd_status pd_denoise_batch(const pd_volume* vols, int32_t n_vols, const pd_param
     w.list = d_list + off;
     w.vols = d_vols;
     w.vol_of = d_volof + off;
+    // this chunk's volumes set its launch shapes (the work list is in volume order)
+    int nc = 0, mc = 0;
+    size_t esm = 0;
+    for (int k = 0; k < n_vols; ++k) {
+      const int64_t f = t.v[k].d.first, c = t.v[k].count;
+      if (c == 0 || f + c <= off || f >= off + cnt) continue;
+      nc = std::max(nc, (int)t.v[k].d.g.cols);
+      mc = std::max(mc, (int)t.v[k].d.g.rows);
+      bool in_smem;
+      esm = std::max(esm, eig_smem_bytes(cplx, (int)t.v[k].d.g.cols, &in_smem));
+    }
+    G.rows = mc;
+    G.cols = nc;
+    ep.rows = mc;
+    ep.cols = nc;
+    ep.smem_bytes = esm;
     launch_patch_mean(G, cplx, nullptr, w, s);
     if (p->method == PD_METHOD_HYBRID || (p->method == PD_METHOD_OPTIMAL && p->has_prior))
       launch_prior(G, p->method, nullptr, w, s);
     launch_gram_fp32(G, cplx, nullptr, w, s);
-    PD_TRY(cuda_check(launch_eig(cplx, n_max, ep, w, s), "eigensolver launch"));
+    PD_TRY(cuda_check(launch_eig(cplx, nc, ep, w, s), "eigensolver launch"));
     SynthArgs sa{};
     sa.recombination = p->recombination;
     sa.list_offset = off;

@@ -1295,6 +1295,7 @@ template <bool CPLX, int NS>
 static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s, const pd_adaptive* ad) {
   bool in_smem;
   size_t smem = eig_smem_bytes(CPLX, n, &in_smem);
+  if (ep.smem_bytes > smem) smem = ep.smem_bytes;  // a batch whose smaller patches fit shared memory
   int flags = in_smem ? 1 : 0;
   if (!CPLX && ep.method == EIG_MODE_TOP1 && in_smem) {
     const size_t q = al16(sizeof(float) * (size_t)((n < LANCZOS_STEPS ? n : LANCZOS_STEPS) + 1) * n);

@@ -17,7 +17,7 @@ constexpr int GK = 16;   // rows per k step
 constexpr int GRAM_THREADS = 256;
 
 template <bool CPLX>
-__global__ void __launch_bounds__(MEAN_THREADS) k_patch_mean(Geo g, const typename Elem<CPLX>::T* in,
+__global__ void __launch_bounds__(MEAN_THREADS) k_patch_mean(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
                                                              PatchWork w) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ int64_t rowbase[];
@@ -95,7 +95,7 @@ __device__ __forceinline__ void tile_pair(int t, int& bi, int& bj) {
 // Register-tiled 64x64 block of C = Xc^H Xc for one patch (grid.x = patch,
 // grid.y = lower tile pair).
 template <bool CPLX>
-__global__ void __launch_bounds__(GRAM_THREADS) k_gram_fp32(Geo g, const typename Elem<CPLX>::T* in,
+__global__ void __launch_bounds__(GRAM_THREADS) k_gram_fp32(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
                                                             PatchWork w) {
   using T = typename Elem<CPLX>::T;
   __shared__ T As[GK][GT];

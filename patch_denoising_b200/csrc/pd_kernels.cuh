@@ -93,6 +93,7 @@ struct EigParams {
   double mp_median;
   const double* d_threshold;  // raw / NORDIC: read the threshold here when not NULL
   int only_unfinished;        // 1: solve only the patches with n_active < 0 (left by k_sub)
+  size_t smem_bytes;          // batched calls: dynamic shared memory for the launch (0: by n)
 };
 constexpr int EIG_MODE_TOP1 = 100;
 // every eigenpair, descending: vectors into w.vec, eigenvalues (true units) into

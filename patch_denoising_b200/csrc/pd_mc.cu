@@ -5,6 +5,8 @@
 //
 // Gaussian entries are generated on the fly (pd_rng.cuh): element (r, c) of
 // draw d is a pure function of (seed, d, r, c).
+#include <algorithm>
+
 #include "pd_common.cuh"
 #include "pd_kernels.cuh"
 #include "pd_profile.cuh"
@@ -178,40 +180,77 @@ __device__ double gamma_mt(double a, uint64_t seed, uint32_t draw, uint32_t i) {
   return dd * boost;  // not reached in practice: the mean
 }
 
-// One CTA per draw: L (d x d, row-major, lower part) into Lbuf, then the packed
-// lower W = L L^T (FP64 sums) into gram.
-__global__ void __launch_bounds__(256) k_wishart(int64_t m, int d, uint64_t seed, float* __restrict__ Lbuf,
-                                                 float* __restrict__ gram, int64_t gram_stride) {
-  const uint32_t draw = blockIdx.x;
-  float* L = Lbuf + (int64_t)draw * d * d;
+// L of every draw (d x d, row-major, lower part): grid-stride over (draw, row,
+// group of four columns); the diagonal by gamma_mt.
+__global__ void __launch_bounds__(256) k_wishart_l(int64_t m, int d, int draws, uint64_t seed,
+                                                   float* __restrict__ Lbuf) {
   const int ng = (d + 3) / 4;
-  for (int t = threadIdx.x; t < d * ng; t += blockDim.x) {
-    const int i = t / ng, cg = t % ng;
-    if (4 * cg >= i) continue;
-    float z[4];
-    normals4(seed, draw, (uint64_t)i, (uint32_t)cg, z);
+  const int64_t items = (int64_t)draws * d * ng;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < items; t += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t draw = (uint32_t)(t / ((int64_t)d * ng));
+    const int rem = (int)(t - (int64_t)draw * d * ng);
+    const int i = rem / ng, cg = rem % ng;
+    float* L = Lbuf + (int64_t)draw * d * d;
+    if (4 * cg < i) {
+      float z[4];
+      normals4(seed, draw, (uint64_t)i, (uint32_t)cg, z);
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
-      if (4 * cg + q < i) L[(int64_t)i * d + 4 * cg + q] = z[q];
-  }
-  for (int i = threadIdx.x; i < d; i += blockDim.x)
-    L[(int64_t)i * d + i] = (float)sqrt(2.0 * gamma_mt(0.5 * (double)(m - i), seed, draw, (uint32_t)i));
-  __syncthreads();
-  float* W = gram + (int64_t)draw * gram_stride;
-  for (int j = 0; j < d; ++j) {
-    const float* lj = L + (int64_t)j * d;
-    for (int i = j + threadIdx.x; i < d; i += blockDim.x) {
-      const float* li = L + (int64_t)i * d;
-      double s = 0.0;
-      for (int k = 0; k <= j; ++k) s += (double)li[k] * lj[k];
-      W[pk(i, j, d)] = (float)s;
+      for (int q = 0; q < 4; ++q)
+        if (4 * cg + q < i) L[(int64_t)i * d + 4 * cg + q] = z[q];
     }
+    if (cg == i / 4)  // the thread of the diagonal's column group
+      L[(int64_t)i * d + i] = (float)sqrt(2.0 * gamma_mt(0.5 * (double)(m - i), seed, draw, (uint32_t)i));
   }
+}
+
+// W = L L^T, packed lower: grid (lower 32 x 32 tile pairs, draws); W_ij =
+// sum_{k <= j} L_ik L_jk through 32-wide K slabs in shared memory.
+constexpr int WT = 32;
+__global__ void __launch_bounds__(256) k_wishart_w(int d, const float* __restrict__ Lbuf, float* __restrict__ gram,
+                                                   int64_t gram_stride) {
+  __shared__ float As[WT][WT + 1], Bs[WT][WT + 1];
+  int bi, bj;
+  mc_tile_pair(blockIdx.x, bi, bj);
+  const int draw = blockIdx.y;
+  const float* L = Lbuf + (int64_t)draw * d * d;
+  const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;  // 2 x 2 outputs per thread
+  float acc[2][2] = {};
+  const int kend = min((bj + 1) * WT, d);  // L_jk = 0 for k > j
+  for (int k0 = 0; k0 < kend; k0 += WT) {
+    for (int e = tid; e < WT * WT; e += 256) {
+      const int r = e / WT, c = e % WT;
+      const int ia = bi * WT + r, ib = bj * WT + r, k = k0 + c;
+      As[r][c] = (ia < d && k <= ia) ? L[(int64_t)ia * d + k] : 0.f;
+      Bs[r][c] = (ib < d && k <= ib) ? L[(int64_t)ib * d + k] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int c = 0; c < WT; ++c) {
+#pragma unroll
+      for (int x = 0; x < 2; ++x)
+#pragma unroll
+        for (int y = 0; y < 2; ++y) acc[x][y] = fmaf(As[ty * 2 + x][c], Bs[tx * 2 + y][c], acc[x][y]);
+    }
+    __syncthreads();
+  }
+  float* W = gram + (int64_t)draw * gram_stride;
+#pragma unroll
+  for (int x = 0; x < 2; ++x)
+#pragma unroll
+    for (int y = 0; y < 2; ++y) {
+      const int i = bi * WT + ty * 2 + x, j = bj * WT + tx * 2 + y;
+      if (i < d && j <= i) W[pk(i, j, d)] = acc[x][y];
+    }
 }
 
 void launch_wishart(int64_t m, int d, int n_iter, uint64_t seed, float* Lbuf, float* gram, int64_t gram_stride,
                     cudaStream_t s) {
-  PD_TIMED("mc_wishart", s, k_wishart<<<n_iter, 256, 0, s>>>(m, d, seed, Lbuf, gram, gram_stride));
+  const int64_t items = (int64_t)n_iter * d * ((d + 3) / 4);
+  const int blocks = (int)std::min<int64_t>((items + 255) / 256, 148 * 8);
+  PD_TIMED("mc_wishart", s, k_wishart_l<<<blocks, 256, 0, s>>>(m, d, n_iter, seed, Lbuf));
+  const int nt = (d + WT - 1) / WT;
+  dim3 grid(nt * (nt + 1) / 2, n_iter);
+  PD_TIMED("mc_wishart", s, k_wishart_w<<<grid, 256, 0, s>>>(d, Lbuf, gram, gram_stride));
 }
 
 }  // namespace pd

@@ -26,7 +26,7 @@ __device__ __forceinline__ void acc_add(cf* p, cf v) {
 // WIDE: with the grouped reduction for ranks above 8 (adaptive launches only;
 // its registers would cost the low-rank methods occupancy).
 template <bool CPLX, int NS, int R, bool WIDE>
-__global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Elem<CPLX>::T* in,
+__global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
                                                        PatchWork w, SynthArgs sa, int ysplit) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ __align__(16) unsigned char sm[];
