@@ -696,8 +696,40 @@ pd_status pd_denoise_batch(const pd_volume* vols, int32_t n_vols, const pd_param
   ep.rows = m_max;
   ep.cols = n_max;
   ep.threshold_scale = p->threshold_scale;
-  for (int64_t off = 0; off < total; off += chunk) {
-    const int cnt = (int)std::min<int64_t>(chunk, total - off);
+  // chunks of at most `chunk` patches that do not mix the kernels' frame-count
+  // classes (their register slots per lane are sized by the largest frame count
+  // of a launch), in work-list order
+  auto frame_class = [](int64_t n) { return n <= 64 ? 0 : n <= 128 ? 1 : n <= 224 ? 2 : n <= 320 ? 3 : 4; };
+  std::vector<std::pair<int64_t, int64_t>> pieces;  // (offset, count)
+  {
+    int64_t start = 0, len = 0;
+    int cls = -1;
+    for (int k = 0; k < n_vols; ++k) {
+      int64_t f = t.v[k].d.first, c = t.v[k].count;
+      if (c == 0) continue;
+      const int kc = frame_class(t.v[k].d.g.cols);
+      if (len > 0 && kc != cls) {
+        pieces.emplace_back(start, len);
+        len = 0;
+      }
+      cls = kc;
+      while (c > 0) {
+        if (len == 0) start = f;
+        const int64_t take = std::min<int64_t>(c, chunk - len);
+        len += take;
+        f += take;
+        c -= take;
+        if (len == chunk) {
+          pieces.emplace_back(start, len);
+          len = 0;
+        }
+      }
+    }
+    if (len > 0) pieces.emplace_back(start, len);
+  }
+  for (const auto& pc : pieces) {
+    const int64_t off = pc.first;
+    const int cnt = (int)pc.second;
     PatchWork w = carve_work(d_ws, cnt, n_max, cplx, &used);
     w.list = d_list + off;
     w.vols = d_vols;

@@ -24,8 +24,10 @@ __device__ __forceinline__ void acc_add(cf* p, cf v) {
 }
 
 // WIDE: with the grouped reduction for ranks above 8 (adaptive launches only;
-// its registers would cost the low-rank methods occupancy).
-template <bool CPLX, int NS, int R, bool WIDE>
+// its registers would cost the low-rank methods occupancy). BATCH: the patch's
+// volume comes from the batched call's table (kept out of the one-volume
+// instantiations, whose registers it would raise from 80 to 97).
+template <bool CPLX, int NS, int R, bool WIDE, bool BATCH>
 __global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
                                                        PatchWork w, SynthArgs sa, int ysplit) {
   using T = typename Elem<CPLX>::T;
@@ -35,7 +37,7 @@ __global__ void __launch_bounds__(SYN_THREADS) k_synth(Geo g, const typename Ele
   // voxels close together in time)
   const int p = (int)(blockIdx.x / (unsigned)ysplit);
   const int yb = (int)(blockIdx.x - (unsigned)p * (unsigned)ysplit);
-  if (w.vols) {  // batched call: this patch's volume and its output buffers
+  if constexpr (BATCH) {  // batched call: this patch's volume and its output buffers
     const VolDesc& v = w.vols[w.vol_of[p]];
     g = v.g;
     in = reinterpret_cast<const T*>(v.in);
@@ -219,7 +221,8 @@ static void synth_ns(const Geo& g, const void* in, const PatchWork& w, const Syn
   constexpr int R = CPLX ? 2 : 4;
   const int n = g.cols;
   const size_t smem = sizeof(T) * ((size_t)SYN_NW * R * n + n) + sizeof(float) * n + 16;
-  auto kern = a.wide ? k_synth<CPLX, NS, R, true> : k_synth<CPLX, NS, R, false>;
+  auto kern = a.wide ? k_synth<CPLX, NS, R, true, false>
+                     : (w.vols ? k_synth<CPLX, NS, R, false, true> : k_synth<CPLX, NS, R, false, false>);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int rows_per_block = SYN_NW * R;
   int ysplit = (g.rows + rows_per_block - 1) / rows_per_block;
