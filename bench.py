@@ -482,7 +482,9 @@ def ours_arm(args, rank, world):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, dist, dev)
     h2d = x.nbytes
-    d2h = out.nbytes + w.nbytes + nm.nbytes + rm.nbytes
+    # bytes that crossed PCIe: a map constant along frames comes back spatial only
+    # (returned as a broadcast view, last stride 0)
+    d2h = sum(a.nbytes // a.shape[-1] if a.strides[-1] == 0 else a.nbytes for a in (out, w, nm, rm))
 
     extras = run_extras(dev, dist) if not args.no_extras else {}
 

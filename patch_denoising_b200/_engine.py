@@ -158,6 +158,11 @@ def _staged_h2d(a: np.ndarray, device) -> torch.Tensor:
 _NP = {torch.float32: np.float32, torch.complex64: np.complex64}
 
 
+def spread_over_frames(spatial, shape):
+    """A read-only 4D view of a map that is constant along frames (no copy)."""
+    return np.broadcast_to(spatial[..., None], shape)
+
+
 def to_host(tensors):
     """Device tensors -> NumPy arrays through pinned buffers (torch's host cache)."""
     hosts = []
@@ -467,11 +472,15 @@ def run_host(
         mc_ws = torch.empty(max(mc_need.value, 1), dtype=torch.uint8, device=device)
         level = torch.empty(2, dtype=torch.float64, device=device)
 
-    # host buffers of the results (pinned, returned as NumPy views)
+    # host buffers of the results (pinned, returned as NumPy views); with one
+    # time window the maps are constant along frames: only their spatial part
+    # crosses PCIe (returned as broadcast views)
     h_out = torch.empty(shape, dtype=tdtype, pin_memory=True)
     h_w = torch.empty(shape, dtype=torch.float32, pin_memory=True)
-    h_nm = torch.empty(shape, dtype=torch.float32, pin_memory=True)
-    h_rm = torch.empty(shape, dtype=torch.int32, pin_memory=True)
+    maps_spatial = ngt == 1
+    nm_spatial = maps_spatial and recombination != "center"  # "center": the centre frame only
+    h_nm = torch.empty(shape[:-1] if nm_spatial else shape, dtype=torch.float32, pin_memory=True)
+    h_rm = torch.empty(shape[:-1] if maps_spatial else shape, dtype=torch.int32, pin_memory=True)
 
     # upload state: the input goes up slab by slab on the copy stream
     src = torch.from_numpy(x.reshape(-1).view(np.uint8))
@@ -543,8 +552,11 @@ def run_host(
             fin.record(comp)
             dnl.wait_event(fin)
             with torch.cuda.stream(dnl):
-                for h, d in ((h_out, out), (h_w, weights), (h_nm, noise_map), (h_rm, rank_map)):
+                for h, d in ((h_out, out), (h_w, weights)):
                     h[x_done:x_end].copy_(d[x_done:x_end], non_blocking=True)
+                for h, d, flat in ((h_nm, noise_map, nm_spatial), (h_rm, rank_map, maps_spatial)):
+                    src = d[x_done:x_end, ..., 0] if flat else d[x_done:x_end]
+                    h[x_done:x_end].copy_(src, non_blocking=True)
             x_done = x_end
     # the compute stream's later work (and buffer reuse) comes after both copy streams
     comp.wait_stream(upl)
@@ -555,4 +567,9 @@ def run_host(
     dnl.synchronize()
     comp.synchronize()
     check_device_errors(block=True)
-    return (h_out.numpy(), h_w.numpy(), h_nm.numpy(), h_rm.numpy()), res
+    nm, rm = h_nm.numpy(), h_rm.numpy()
+    if nm_spatial:
+        nm = spread_over_frames(nm, shape)
+    if maps_spatial:
+        rm = spread_over_frames(rm, shape)
+    return (h_out.numpy(), h_w.numpy(), nm, rm), res

@@ -182,8 +182,19 @@ class BaseSpaceTimeDenoiser(abc.ABC):
             if in_dtype in (torch.float64, torch.complex128):
                 out = out.to(in_dtype)
             return out, res.weights, res.noise_map, res.rank_map
+        # one time window (a patch spans every frame): the maps are constant
+        # along frames, so only their spatial part is copied back
+        # (the noise map of "center" recombination sits at the centre frame only)
+        one_window = p_s[-1] >= shape[-1]
+        nm_flat = one_window and self.recombination != "center"
+        nm_d = res.noise_map[..., 0] if nm_flat else res.noise_map
+        rm_d = res.rank_map[..., 0] if one_window else res.rank_map
         out, weights, noise_map, rank_map, pidx, prank, pnoise = _engine.to_host(
-            [res.out, res.weights, res.noise_map, res.rank_map, res.patch_index, res.patch_rank, res.patch_noise])
+            [res.out, res.weights, nm_d, rm_d, res.patch_index, res.patch_rank, res.patch_noise])
+        if nm_flat:
+            noise_map = _engine.spread_over_frames(noise_map, shape)
+        if one_window:
+            rank_map = _engine.spread_over_frames(rank_map, shape)
         if np.dtype(in_dtype) != out.dtype:
             out = out.astype(in_dtype)
         self.patch_index_, self.patch_rank_, self.patch_noise_ = pidx, prank, pnoise
