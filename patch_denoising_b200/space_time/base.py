@@ -184,9 +184,10 @@ class BaseSpaceTimeDenoiser(abc.ABC):
             return out, res.weights, res.noise_map, res.rank_map
         # one time window (a patch spans every frame): the maps are constant
         # along frames, so only their spatial part is copied back
-        # (the noise map of "center" recombination sits at the centre frame only)
+        # (the noise map of "center" recombination sits at the centre frame only,
+        # and a 4D mask zeroes it frame by frame)
         one_window = p_s[-1] >= shape[-1]
-        nm_flat = one_window and self.recombination != "center"
+        nm_flat = one_window and self.recombination != "center" and (m is None or m.dim() < len(shape))
         nm_d = res.noise_map[..., 0] if nm_flat else res.noise_map
         rm_d = res.rank_map[..., 0] if one_window else res.rank_map
         out, weights, noise_map, rank_map, pidx, prank, pnoise = _engine.to_host(
