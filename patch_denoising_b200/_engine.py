@@ -555,8 +555,8 @@ def run_host(
                 for h, d in ((h_out, out), (h_w, weights)):
                     h[x_done:x_end].copy_(d[x_done:x_end], non_blocking=True)
                 for h, d, flat in ((h_nm, noise_map, nm_spatial), (h_rm, rank_map, maps_spatial)):
-                    src = d[x_done:x_end, ..., 0] if flat else d[x_done:x_end]
-                    h[x_done:x_end].copy_(src, non_blocking=True)
+                    piece = d[x_done:x_end, ..., 0] if flat else d[x_done:x_end]
+                    h[x_done:x_end].copy_(piece, non_blocking=True)
             x_done = x_end
     # the compute stream's later work (and buffer reuse) comes after both copy streams
     comp.wait_stream(upl)
