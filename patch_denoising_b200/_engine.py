@@ -294,7 +294,8 @@ def run(
     out = torch.zeros(shape, dtype=data.dtype, device=device)
     wacc = torch.zeros(nvox * int(g.grid[3]), dtype=torch.float32, device=device)
     nacc = torch.zeros_like(wacc)
-    nctr = torch.zeros(shape, dtype=torch.float32, device=device)
+    # the centre-element noise map is read and written by "center" recombination only
+    nctr = torch.zeros(shape if recombination == "center" else (1,), dtype=torch.float32, device=device)
     rank_map = torch.zeros(shape, dtype=torch.int32, device=device)
     prank = torch.zeros(max(n_sel, 1), dtype=torch.int32, device=device)
     pnoise = torch.zeros(max(n_sel, 1), dtype=torch.float32, device=device)
@@ -458,7 +459,7 @@ def run_host(
     out = torch.zeros(shape, dtype=tdtype, device=device)
     wacc = torch.zeros(nvox * ngt, dtype=torch.float32, device=device)
     nacc = torch.zeros_like(wacc)
-    nctr = torch.zeros(shape, dtype=torch.float32, device=device)
+    nctr = torch.zeros(shape if recombination == "center" else (1,), dtype=torch.float32, device=device)
     rank_map = torch.zeros(shape, dtype=torch.int32, device=device)
     weights = torch.empty(shape, dtype=torch.float32, device=device)
     noise_map = torch.empty(shape, dtype=torch.float32, device=device)
@@ -546,7 +547,8 @@ def run_host(
             _lib.check(lib.pd_finalize(
                 ctypes.byref(sub), pp, ctypes.c_void_p(out.data_ptr() + e0 * out.element_size()),
                 ctypes.c_void_p(wacc.data_ptr() + 4 * v0 * ngt), ctypes.c_void_p(nacc.data_ptr() + 4 * v0 * ngt),
-                ctypes.c_void_p(nctr.data_ptr() + 4 * e0), ctypes.c_void_p(weights.data_ptr() + 4 * e0),
+                ctypes.c_void_p(nctr.data_ptr() + (4 * e0 if recombination == "center" else 0)),
+                ctypes.c_void_p(weights.data_ptr() + 4 * e0),
                 ctypes.c_void_p(noise_map.data_ptr() + 4 * e0), None, 0, s))
             fin = torch.cuda.Event()
             fin.record(comp)

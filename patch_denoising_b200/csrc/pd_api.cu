@@ -159,6 +159,28 @@ double mp_cdf(double x, double beta) {
   return (G(x) - G(a)) / (2.0 * M_PI * beta);
 }
 
+// A non-blocking side stream with its fork and join events, per device and
+// host thread (created on first use, kept for the thread's lifetime).
+struct SideStream {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+pd_status side_stream(SideStream** out) {
+  static thread_local SideStream per_dev[64];
+  int dev = 0;
+  PD_TRY(cuda_check(cudaGetDevice(&dev), "current device"));
+  if (dev < 0 || dev >= 64) return fail(PD_ERR_UNSUPPORTED, "device index %d", dev);
+  SideStream& ss = per_dev[dev];
+  if (!ss.stream) {
+    PD_TRY(cuda_check(cudaStreamCreateWithFlags(&ss.stream, cudaStreamNonBlocking), "side stream"));
+    PD_TRY(cuda_check(cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming), "fork event"));
+    PD_TRY(cuda_check(cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming), "join event"));
+  }
+  *out = &ss;
+  return PD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -332,7 +354,7 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
                                       void* d_out_acc, float* d_weight_acc, float* d_noise_acc, float* d_noise_ctr,
                                       int32_t* d_rank_map, int32_t* d_patch_rank, float* d_patch_noise, void* d_ws,
                                       size_t ws_bytes, void* stream, const double* d_thr,
-                                      const pd_adaptive* ad = nullptr) {
+                                      const pd_adaptive* ad = nullptr, cudaEvent_t eig_after = nullptr) {
   PD_TRY(check_geometry(g));
   PD_TRY(check_params(g, p));
   if ((p->method == PD_METHOD_ADAPTIVE) != (ad != nullptr))
@@ -381,6 +403,8 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
       PD_TRY(cuda_check(launch_gram_packed(G, cplx, d_in, w, w.packed, s), "tensor-core Gram launch"));
     else
       launch_gram_fp32(G, cplx, d_in, w, s);
+    if (eig_after && off == 0)  // the threshold comes from work on another stream
+      PD_TRY(cuda_check(cudaStreamWaitEvent(s, eig_after, 0), "join the Monte-Carlo stream"));
     if (p->precision == PD_PRECISION_MIXED && p->method == PD_METHOD_RAW && sub_supported(cplx, n, (int)g->rows)) {
       // the subspace solver for the patches it certifies, the full solver for the rest
       PD_TRY(cuda_check(launch_sub(cplx, n, ep, w, s), "subspace eigensolver launch"));
@@ -507,17 +531,34 @@ pd_status pd_nordic_denoise_patches(const pd_geometry* g, const pd_params* p, do
   if (!d_level) return fail(PD_ERR_INVALID, "NULL level output");
   cudaStream_t s = (cudaStream_t)stream;
   if (mc_rows < 0) return fail(PD_ERR_INVALID, "negative Monte-Carlo row count");
+  cudaEvent_t joined = nullptr;
   if (mc_rows > 0) {
-    // the draws, their Grams and top-1 eigenvalues, then the level and the threshold on the device
+    // the draws, their Grams and top-1 eigenvalues, then the level and the
+    // threshold on the device. On the chosen path this chain is a few small
+    // launches on about ten SMs, so it runs on a side stream beside the patch
+    // means, packing and Grams, and the eigensolver waits for it.
+    cudaStream_t ms = s;
+    if (p->precision == PD_PRECISION_MIXED) {
+      SideStream* side = nullptr;
+      PD_TRY(side_stream(&side));
+      PD_TRY(cuda_check(cudaEventRecord(side->fork, s), "fork the Monte-Carlo stream"));
+      PD_TRY(cuda_check(cudaStreamWaitEvent(side->stream, side->fork, 0), "fork the Monte-Carlo stream"));
+      ms = side->stream;
+      joined = side->join;
+    }
     PatchWork mw;
-    PD_TRY(mc_launch(mc_rows, g->cols, n_iter, seed, p->precision, d_mc_ws, mc_ws_bytes, s, &mw));
-    launch_mc_level(mw.prior, n_iter, noise_std, d_level, s);
+    PD_TRY(mc_launch(mc_rows, g->cols, n_iter, seed, p->precision, d_mc_ws, mc_ws_bytes, ms, &mw));
+    launch_mc_level(mw.prior, n_iter, noise_std, d_level, ms);
     PD_TRY(cuda_check(cudaGetLastError(), "Monte-Carlo level launch"));
+    if (joined) PD_TRY(cuda_check(cudaEventRecord(joined, ms), "join the Monte-Carlo stream"));
   }
   // the patch loop reads the threshold from d_level[1]
-  return denoise_patches_impl(g, p, d_in, nullptr, d_patch_list, n_selected, d_out_acc, d_weight_acc, d_noise_acc,
-                              d_noise_ctr, d_rank_map, d_patch_rank, d_patch_noise, d_ws, ws_bytes, stream,
-                              d_level + 1);
+  const pd_status st = denoise_patches_impl(g, p, d_in, nullptr, d_patch_list, n_selected, d_out_acc, d_weight_acc,
+                                            d_noise_acc, d_noise_ctr, d_rank_map, d_patch_rank, d_patch_noise, d_ws,
+                                            ws_bytes, stream, d_level + 1, nullptr, joined);
+  if (joined && n_selected == 0)  // nothing waited for the side stream: join it here
+    PD_TRY(cuda_check(cudaStreamWaitEvent(s, joined, 0), "join the Monte-Carlo stream"));
+  return st;
 }
 
 pd_status pd_adaptive_qut_level(int64_t rows, int64_t cols, int32_t n_sim, uint64_t seed, int32_t precision,
