@@ -98,3 +98,17 @@ def load_adaptive_golden(name):
 @pytest.fixture(scope="session")
 def golden():
     return {n: load_golden(n) for n in golden_names()}
+
+
+def pytest_terminal_summary(terminalreporter):
+    """Print the near-threshold rank ties of the GPU parity comparisons."""
+    parity = sys.modules.get("parity")
+    log = getattr(parity, "TIE_LOG", None)
+    if not log:
+        return
+    tied = [r for r in log if r[2]]
+    terminalreporter.write_line(
+        f"parity: {len(log)} comparisons, {sum(r[2] for r in log)} rank ties in {len(tied)} of them "
+        f"(bands: {parity.TIE_TOL})")
+    for test, precision, n, margin in tied:
+        terminalreporter.write_line(f"  {test} [{precision}]: {n} ties, largest margin {margin:.3g}")

@@ -2,6 +2,8 @@
 
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 import oracle
@@ -14,8 +16,13 @@ from patch_denoising_b200.space_time import (
 )
 
 # Decision margins below these (relative) are near-threshold ties: the rank may
-# differ from the FP64 oracle there, and the oracle then replays our rank.
-TIE_TOL = {"fp32": 2e-3, "mixed": 2e-2}
+# differ from the FP64 oracle there, and the oracle then replays our rank. The
+# mixed band is 5x the largest relative eigenvalue error of the split-bf16 Gram
+# measured on the parity volumes (1.9e-3; tests/test_mixed_tie_bound.py).
+TIE_TOL = {"fp32": 2e-3, "mixed": 1e-2}
+# (test id, precision, ties, largest tie margin) of every compare() call, printed
+# in the terminal summary
+TIE_LOG = []
 # rel-L2 bounds against the FP64 oracle: 1e-5 for plain FP32, 1e-4 for the mixed path
 OUT_TOL = {"fp32": 1e-5, "mixed": 1e-4}
 
@@ -87,6 +94,8 @@ def compare(call, x, precision="fp32", nordic_max_sval=None, report=None):
         ties[int(ref["patches"][j])] = int(ours_rank[j])
     if ties:
         ref = run_oracle(call, x, rank_override=ties, threshold=thr)
+    TIE_LOG.append((os.environ.get("PYTEST_CURRENT_TEST", "?").split(" ")[0], precision, len(ties),
+                    max((float(ref["patch_margin"][j]) for j in diff), default=0.0)))
     gold = ref["out"]
     np.testing.assert_array_equal(np.isnan(out), np.isnan(gold))
     err_out = rel_l2(out.astype(gold.dtype), gold)
