@@ -497,6 +497,8 @@ def ours_arm(args, rank, world):
         if pk_path.exists():
             peaks = json.loads(pk_path.read_text())
         for name, (nl, tot) in sorted(kern.items(), key=lambda kv: -kv[1][1]):
+            if name in ("eig", "eig_sub16") and "eig_sub8" in kern:
+                continue  # they take only the patches the P=8 pass left uncertified (none here): no fixed count
             work, kind = algorithmic(name, n_p, M, n, ranks)
             if work is None:
                 continue
