@@ -132,7 +132,7 @@ def to_device(x, device, dtype=None) -> torch.Tensor:
 # buffers: the host copy of chunk k + 1 (torch's multi-threaded memcpy) overlaps
 # the DMA of chunk k, instead of the driver's single-threaded staging.
 _STAGE_MIN = 16 << 20
-_STAGE_CHUNK = 32 << 20
+_STAGE_CHUNK = 16 << 20
 
 
 def _staged_h2d(a: np.ndarray, device) -> torch.Tensor:
@@ -369,6 +369,8 @@ def estimate_noise(data: torch.Tensor, block_size: int) -> torch.Tensor:
 # the next range runs. Uploads and downloads each have a stream of their own.
 STREAM_MIN_BYTES = 64 << 20
 _copy_streams = {}
+# bytes the last streamed call moved over PCIe (host to device, device to host)
+LAST_TRANSFER = {"h2d": 0, "d2h": 0}
 
 
 def _copy_stream(device, which):
@@ -479,6 +481,12 @@ def run_host(
     h_out = torch.empty(shape, dtype=tdtype, pin_memory=True)
     h_w = torch.empty(shape, dtype=torch.float32, pin_memory=True)
     maps_spatial = ngt == 1
+    # with one time window the weights are constant along frames too: their
+    # spatial part comes down and is spread over the frames of the returned
+    # (full, writable) array on the host, while the output is still in flight
+    h_w_sp = torch.empty(shape[:-1], dtype=torch.float32, pin_memory=True) if maps_spatial else None
+    w_slabs = []
+    d2h = 0
     nm_spatial = maps_spatial and recombination != "center"  # "center": the centre frame only
     h_nm = torch.empty(shape[:-1] if nm_spatial else shape, dtype=torch.float32, pin_memory=True)
     h_rm = torch.empty(shape[:-1] if maps_spatial else shape, dtype=torch.int32, pin_memory=True)
@@ -512,10 +520,21 @@ def run_host(
             ev = done[b]
         return ev
 
+    # ranges of x positions, each at most one eigensolver wave. The first is a
+    # single position, so the first download starts once a sixth of the input
+    # is up; so is the last, so the final slab (everything the last range
+    # completes) is small and its download short once the last input has landed
+    bounds = [(0, 1)] if gx > 2 else []
+    a = bounds[-1][1] if bounds else 0
+    while a < gx:
+        bounds.append((a, min(gx, a + xs_per)))
+        a = bounds[-1][1]
+    if bounds[-1][1] - bounds[-1][0] > 1:
+        a, b_ = bounds.pop()
+        bounds += [(a, b_ - 1), (b_ - 1, b_)]
     words = []
     x_done = 0
-    for a in range(0, gx, xs_per):
-        b_ = min(gx, a + xs_per)
+    for a, b_ in bounds:
         first, cnt = a * per_x, (b_ - a) * per_x
         ev = upload_to(((b_ - 1) * step_x + patch_x) * slab)
         if ev is not None:
@@ -554,12 +573,25 @@ def run_host(
             fin.record(comp)
             dnl.wait_event(fin)
             with torch.cuda.stream(dnl):
-                for h, d in ((h_out, out), (h_w, weights)):
-                    h[x_done:x_end].copy_(d[x_done:x_end], non_blocking=True)
+                if maps_spatial:  # first, so that its spreading overlaps the output's download
+                    h_w_sp[x_done:x_end].copy_(weights[x_done:x_end, ..., 0], non_blocking=True)
+                    ev_w = torch.cuda.Event()
+                    ev_w.record(dnl)
+                    w_slabs.append((x_done, x_end, ev_w))
+                else:
+                    h_w[x_done:x_end].copy_(weights[x_done:x_end], non_blocking=True)
+                h_out[x_done:x_end].copy_(out[x_done:x_end], non_blocking=True)
                 for h, d, flat in ((h_nm, noise_map, nm_spatial), (h_rm, rank_map, maps_spatial)):
                     piece = d[x_done:x_end, ..., 0] if flat else d[x_done:x_end]
                     h[x_done:x_end].copy_(piece, non_blocking=True)
+            d2h += out[x_done:x_end].nbytes + (h_w_sp[x_done:x_end] if maps_spatial else h_w[x_done:x_end]).nbytes
+            d2h += h_nm[x_done:x_end].nbytes + h_rm[x_done:x_end].nbytes
             x_done = x_end
+    # spread each slab's spatial weights over the frames as soon as it has landed
+    # (torch's multithreaded host copy; the output slabs are still coming down)
+    for x0, x1, ev_w in w_slabs:
+        ev_w.synchronize()
+        h_w[x0:x1].copy_(h_w_sp[x0:x1, ..., None].expand(x1 - x0, *shape[1:]))
     # the compute stream's later work (and buffer reuse) comes after both copy streams
     comp.wait_stream(upl)
     comp.wait_stream(dnl)
@@ -569,6 +601,7 @@ def run_host(
     dnl.synchronize()
     comp.synchronize()
     check_device_errors(block=True)
+    LAST_TRANSFER.update(h2d=int(x.nbytes), d2h=int(d2h))
     nm, rm = h_nm.numpy(), h_rm.numpy()
     if nm_spatial:
         nm = spread_over_frames(nm, shape)

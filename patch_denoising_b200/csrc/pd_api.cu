@@ -105,9 +105,18 @@ size_t work_bytes(int count, int n, bool cplx, size_t packed_per_patch = 0) {
   return used;
 }
 
+// The mixed path synthesises high-rank patches (the adaptive rules keep whole
+// spectra) on the tensor cores; center recombination writes one row per patch
+// and keeps the SIMT kernel.
+bool synth_tc_used(const pd_params* p) {
+  return p->precision == PD_PRECISION_MIXED && p->method == PD_METHOD_ADAPTIVE &&
+         p->recombination != PD_RECOMB_CENTER;
+}
+
 size_t packed_of(const pd_geometry* g, const pd_params* p) {
-  return p->precision == PD_PRECISION_MIXED ? packed_bytes_per_patch((int)g->cols, p->is_complex != 0, (int)g->rows)
-                                            : 0;
+  return p->precision == PD_PRECISION_MIXED
+             ? packed_bytes_per_patch((int)g->cols, p->is_complex != 0, (int)g->rows, synth_tc_used(p))
+             : 0;
 }
 
 pd_status check_geometry(const pd_geometry* g) {
@@ -399,8 +408,9 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
     if (p->method == PD_METHOD_HYBRID || p->method == PD_METHOD_ADAPTIVE ||
         (p->method == PD_METHOD_OPTIMAL && p->has_prior))
       launch_prior(G, p->method, d_noise_std, w, s);
+    const bool tc_synth = synth_tc_used(p);
     if (p->precision == PD_PRECISION_MIXED)
-      PD_TRY(cuda_check(launch_gram_packed(G, cplx, d_in, w, w.packed, s), "tensor-core Gram launch"));
+      PD_TRY(cuda_check(launch_gram_packed(G, cplx, d_in, w, w.packed, s, tc_synth), "tensor-core Gram launch"));
     else
       launch_gram_fp32(G, cplx, d_in, w, s);
     if (eig_after && off == 0)  // the threshold comes from work on another stream
@@ -426,7 +436,10 @@ static pd_status denoise_patches_impl(const pd_geometry* g, const pd_params* p, 
     sa.list_offset = off;
     sa.wide = p->method == PD_METHOD_ADAPTIVE ? 1 : 0;
     sa.row_blocks = 0;
-    launch_synth(G, cplx, d_in, w, sa, s);
+    if (tc_synth)
+      PD_TRY(cuda_check(launch_synth_tc(G, cplx, w, sa, s), "tensor-core synthesis launch"));
+    else
+      launch_synth(G, cplx, d_in, w, sa, s);
     PD_TRY(cuda_check(cudaGetLastError(), "pd_denoise_patches launch"));
   }
   return PD_OK;

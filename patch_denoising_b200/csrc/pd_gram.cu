@@ -16,12 +16,21 @@ constexpr int GT = 64;   // Gram tile edge
 constexpr int GK = 16;   // rows per k step
 constexpr int GRAM_THREADS = 256;
 
+// grid: patches x 64-column chunks, flattened patch-major; 256 threads = 64
+// columns x 4 row groups. A thread sums the rows r = group (mod 4) of its column
+// with two FP64 partial sums (more loads in flight); the groups' sums combine
+// in a fixed order, so the mean is deterministic.
+constexpr int MEAN_COLS = 64;
+constexpr int MEAN_GROUPS = MEAN_THREADS / MEAN_COLS;
+
 template <bool CPLX>
 __global__ void __launch_bounds__(MEAN_THREADS) k_patch_mean(Geo g, const typename Elem<CPLX>::T* __restrict__ in,
-                                                             PatchWork w) {
+                                                             PatchWork w, int chunks) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ int64_t rowbase[];
-  const int p = blockIdx.x;
+  __shared__ double part[MEAN_GROUPS][MEAN_COLS][2];
+  const int p = (int)(blockIdx.x / (unsigned)chunks);
+  const int c0 = (int)(blockIdx.x - (unsigned)p * (unsigned)chunks) * MEAN_COLS;
   if (w.vols) {  // batched call: this patch's volume
     const VolDesc& v = w.vols[w.vol_of[p]];
     g = v.g;
@@ -31,29 +40,57 @@ __global__ void __launch_bounds__(MEAN_THREADS) k_patch_mean(Geo g, const typena
   int64_t o[4];
   patch_origin(g, idx, o);
   const int M = g.rows, n = g.cols;
+  if (c0 >= n) return;  // a batched chunk sized for a longer volume
   for (int r = threadIdx.x; r < M; r += blockDim.x) rowbase[r] = row_voxel(g, o, r) * g.shape[3] + o[3];
   __syncthreads();
-  T* mean = reinterpret_cast<T*>(w.mean) + (int64_t)p * w.n_stride;
-  for (int t = threadIdx.x; t < n; t += blockDim.x) {
-    double sx = 0.0, sy = 0.0;
-    for (int r = 0; r < M; ++r) {
-      const T v = in[rowbase[r] + t];
+  const int c = threadIdx.x % MEAN_COLS, grp = threadIdx.x / MEAN_COLS;
+  const int t = c0 + c;
+  double sx[2] = {0.0, 0.0}, sy[2] = {0.0, 0.0};
+  if (t < n) {
+    int r = grp;
+    for (; r + MEAN_GROUPS < M; r += 2 * MEAN_GROUPS) {
+      const T a = in[rowbase[r] + t];
+      const T b = in[rowbase[r + MEAN_GROUPS] + t];
       if constexpr (CPLX) {
-        sx += v.x;
-        sy += v.y;
+        sx[0] += a.x;
+        sy[0] += a.y;
+        sx[1] += b.x;
+        sy[1] += b.y;
       } else {
-        sx += v;
+        sx[0] += a;
+        sx[1] += b;
       }
     }
+    if (r < M) {
+      const T a = in[rowbase[r] + t];
+      if constexpr (CPLX) {
+        sx[0] += a.x;
+        sy[0] += a.y;
+      } else {
+        sx[0] += a;
+      }
+    }
+  }
+  part[grp][c][0] = sx[0] + sx[1];
+  part[grp][c][1] = sy[0] + sy[1];
+  __syncthreads();
+  if (grp == 0 && t < n) {
+    double ax = part[0][c][0], ay = part[0][c][1];
+#pragma unroll
+    for (int q = 1; q < MEAN_GROUPS; ++q) {
+      ax += part[q][c][0];
+      ay += part[q][c][1];
+    }
+    T* mean = reinterpret_cast<T*>(w.mean) + (int64_t)p * w.n_stride;
     if constexpr (CPLX) {
-      mean[t] = cf{(float)(sx / M), (float)(sy / M)};
+      mean[t] = cf{(float)(ax / M), (float)(ay / M)};
     } else {
-      mean[t] = (float)(sx / M);
+      mean[t] = (float)(ax / M);
     }
     // A NaN or infinite sample makes the sum non-finite (float samples cannot
     // overflow an FP64 sum): the reference's LAPACK calls reject such a patch
     // ("array must not contain infs or NaNs"), so flag it.
-    if (!isfinite(sx) || !isfinite(sy)) atomicExch(w.err, PD_DEVERR_NONFINITE);
+    if (!isfinite(ax) || !isfinite(ay)) atomicExch(w.err, PD_DEVERR_NONFINITE);
   }
 }
 
@@ -190,10 +227,12 @@ void launch_patch_mean(const Geo& g, bool cplx, const void* in, const PatchWork&
     cudaFuncSetAttribute(k_patch_mean<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_patch_mean<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   }
+  const int chunks = (g.cols + MEAN_COLS - 1) / MEAN_COLS;
+  const unsigned grid = (unsigned)((int64_t)w.count * chunks);
   if (cplx)
-    PD_TIMED("patch_mean", s, k_patch_mean<true><<<w.count, MEAN_THREADS, smem, s>>>(g, (const cf*)in, w));
+    PD_TIMED("patch_mean", s, k_patch_mean<true><<<grid, MEAN_THREADS, smem, s>>>(g, (const cf*)in, w, chunks));
   else
-    PD_TIMED("patch_mean", s, k_patch_mean<false><<<w.count, MEAN_THREADS, smem, s>>>(g, (const float*)in, w));
+    PD_TIMED("patch_mean", s, k_patch_mean<false><<<grid, MEAN_THREADS, smem, s>>>(g, (const float*)in, w, chunks));
 }
 
 void launch_prior(const Geo& g, int method, const double* ns, const PatchWork& w, cudaStream_t s) {

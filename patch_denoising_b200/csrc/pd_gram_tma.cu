@@ -6,7 +6,11 @@
 //   rounded up to 64, zero padded), x = hi + lo to about 16 bits. Reads are
 //   coalesced along frames, writes along voxels through a shared-memory
 //   transpose; the kernel is memory bound and runs at full occupancy.
-// k_gram_tma: CTA = (patch, 128 x <=256 block of the lower Gram).
+// k_gram_tma: CTA = (patch, 128 x <=256 block of the lower Gram). When N is
+//   not a multiple of 128 (N = 400 for 200 complex frames), the last, partial
+//   128-row block would compute mostly padding: its rows are produced instead
+//   as a strip of columns, G[0:N, Nmain:N] (Nmain = N rounded down to 128), by
+//   symmetry, from a narrow B box (the remainder rows only).
 //   One thread issues cp.async.bulk.tensor loads (128-byte swizzle, the
 //   canonical K-major layout of tcgen05) into a 2-stage ring guarded by
 //   mbarriers with transaction counts; one thread issues tcgen05.mma with the
@@ -31,7 +35,8 @@ constexpr int PK_C = 64;  // columns per pack tile
 constexpr int TM_BM = 128;
 constexpr int TM_BN = 256;
 constexpr int TM_BOX = 128;  // rows per TMA box
-constexpr int TM_STAGES = 2;
+constexpr int TM_STAGES = 2;      // stages of a full-width block
+constexpr int TM_MAX_STAGES = 6;  // a strip block's narrow stages fit more in the same area
 constexpr int TM_THREADS = 128;
 constexpr uint32_t TM_TILE_A = TM_BM * 128;
 constexpr uint32_t TM_TILE_B = TM_BN * 128;
@@ -60,7 +65,8 @@ __device__ __forceinline__ void pack_store(__nv_bfloat16* hi, __nv_bfloat16* lo,
 __global__ void __launch_bounds__(256) k_pack_patches(Geo g, const float* __restrict__ in, int N, int cplx,
                                                       const float* __restrict__ mean, const int32_t* __restrict__ list,
                                                       __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo,
-                                                      int64_t kp, int ks) {
+                                                      int64_t kp, int ks, __nv_bfloat16* __restrict__ rhi,
+                                                      __nv_bfloat16* __restrict__ rlo, int64_t kn) {
   __shared__ float tile[PK_R][PK_C + 1];
   __shared__ int64_t rbs[2][PK_R];
   const int kt_all = (int)(kp / PK_R), ct = (N + PK_C - 1) / PK_C;
@@ -119,6 +125,14 @@ __global__ void __launch_bounds__(256) k_pack_patches(Geo g, const float* __rest
       const int64_t off = (int64_t)colw * kp + r0 + 2 * lane;
       pack_store(hp, lp, off, tile[2 * lane][cc], tile[2 * lane + 1][cc]);
     }
+    if (rhi) {
+      // the row-major copy for the tensor-core synthesis: 64 columns (128 B) of
+      // a row per warp step, zeros past N (the tile holds zeros there)
+      for (int rr = warp; rr < PK_R; rr += 8) {
+        const int64_t off = ((int64_t)p * kp + r0 + rr) * kn + c0 + 2 * lane;
+        pack_store(rhi, rlo, off, tile[rr][2 * lane], tile[rr][2 * lane + 1]);
+      }
+    }
   }
 }
 
@@ -127,6 +141,8 @@ __global__ void __launch_bounds__(256) k_pack_patches(Geo g, const float* __rest
 // ---------------------------------------------------------------------------
 struct TmaArgs {
   int N;       // real columns of X (= rows of the packed operand)
+  int nmain;   // rows covered by whole 128-row blocks when strips are used (else N)
+  int sbox;    // rows of the strip's B box (the remainder rounded up to 16), 0 without strips
   int n_out;   // output order (N or N/2 for complex)
   int cplx;
   int split;   // 3: hi/lo, 1: hi only
@@ -137,52 +153,61 @@ struct TmaArgs {
   int* err;
 };
 
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2,
-                                            uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
-      : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void tm_block_of(int idx, int N, int& rb, int& nb, int& ncols) {
-  for (rb = 0;; ++rb) {
-    const int lim = min((rb + 1) * TM_BM, N);
+// Block idx of a patch: A rows from arow, B rows from brow, ncols valid
+// columns; strip blocks take B from the narrow map.
+struct TmBlock {
+  int arow, brow, ncols, strip;
+};
+__host__ __device__ inline TmBlock tm_block_of(int idx, int N, int nmain) {
+  for (int rb = 0; rb * TM_BM < nmain; ++rb) {
+    const int lim = min((rb + 1) * TM_BM, nmain == N ? N : nmain);
     const int nbs = (lim + TM_BN - 1) / TM_BN;
-    if (idx < nbs) {
-      nb = idx;
-      ncols = min(lim - nb * TM_BN, TM_BN);
-      return;
-    }
+    if (idx < nbs) return TmBlock{rb * TM_BM, idx * TM_BN, min(lim - idx * TM_BN, TM_BN), 0};
     idx -= nbs;
   }
+  return TmBlock{idx * TM_BM, nmain, N - nmain, 1};  // strip: rows idx*128.., columns nmain..N
+}
+
+__host__ __device__ inline int tm_blocks(int N, int nmain) {
+  int t = 0;
+  for (int rb = 0; rb * TM_BM < nmain; ++rb) {
+    const int lim = min((rb + 1) * TM_BM, nmain == N ? N : nmain);
+    t += (lim + TM_BN - 1) / TM_BN;
+  }
+  if (nmain < N) t += (N + TM_BM - 1) / TM_BM;
+  return t;
 }
 
 __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constant__ CUtensorMap map_hi,
-                                                             const __grid_constant__ CUtensorMap map_lo, TmaArgs a) {
+                                                             const __grid_constant__ CUtensorMap map_lo,
+                                                             const __grid_constant__ CUtensorMap smap_hi,
+                                                             const __grid_constant__ CUtensorMap smap_lo, TmaArgs a) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = a.N;
   const bool split = a.split == 3;
-  const uint32_t stage_bytes = (split ? 2u : 1u) * (TM_TILE_A + TM_TILE_B);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + TM_STAGES * stage_bytes);
+  const uint32_t stage_area = TM_STAGES * (split ? 2u : 1u) * (TM_TILE_A + TM_TILE_B);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + stage_area);
   uint64_t* full = bars;
-  uint64_t* empty = bars + TM_STAGES;
-  uint64_t* done = bars + 2 * TM_STAGES;
+  uint64_t* empty = bars + TM_MAX_STAGES;
+  uint64_t* done = bars + 2 * TM_MAX_STAGES;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
 
   // The Gram blocks that read the same operand rows (of one patch) are
   // consecutive in the flattened grid (patch, block), so they share those rows in L2.
   const int bidx = (int)(blockIdx.x % (unsigned)a.nblk);
   const int pidx = (int)(blockIdx.x / (unsigned)a.nblk);
-  int rb, nb, ncols;
-  tm_block_of(bidx, N, rb, nb, ncols);
+  const TmBlock blk = tm_block_of(bidx, N, a.nmain);
+  const int ncols = blk.ncols;
   const int npad = (ncols + 15) & ~15;
-  const int nbox = (npad + TM_BOX - 1) / TM_BOX;  // B boxes of 128 rows
+  const int nbox = blk.strip ? 1 : (npad + TM_BOX - 1) / TM_BOX;  // B boxes of 128 rows (strip: one narrow box)
+  const uint32_t bbox_bytes = blk.strip ? (uint32_t)a.sbox * 128u : (uint32_t)TM_BOX * 128u;
+  // a stage holds A and B (hi, then lo); a strip's B is narrow, so its ring is
+  // deeper (its MMAs are short and its loads must be in flight to hide latency)
+  const uint32_t b_region = blk.strip ? bbox_bytes : TM_TILE_B;
+  const uint32_t stage_bytes = (split ? 2u : 1u) * (TM_TILE_A + b_region);
+  const int nst = min(TM_MAX_STAGES, (int)(stage_area / stage_bytes));
   uint32_t tcols = 32;
   while (tcols < (uint32_t)npad) tcols <<= 1;
 
@@ -190,10 +215,10 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
   const int zc = pidx;  // third tensor-map coordinate: the patch
   float* out = a.out + (int64_t)pidx * a.out_stride;
   const int nch = (int)((k_end - k_begin + 63) / 64);
-  const uint32_t tx_bytes = (split ? 2u : 1u) * (TM_TILE_A + (uint32_t)nbox * TM_BOX * 128u);
+  const uint32_t tx_bytes = (split ? 2u : 1u) * (TM_TILE_A + (uint32_t)nbox * bbox_bytes);
 
   if (tid == 0) {
-    for (int s = 0; s < TM_STAGES; ++s) {
+    for (int s = 0; s < nst; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -211,9 +236,10 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
 
   if (warp == 0 && lane == 0) {
     // ------------------------------------------------------------ TMA producer
-    for (int c = 0; c < nch; ++c) {
-      const int s = c % TM_STAGES;
-      if (c >= TM_STAGES && !mbar_wait(&empty[s], ((c / TM_STAGES) - 1) & 1)) {
+    int c = 0;
+    for (; c < nch; ++c) {
+      const int s = c % nst;
+      if (c >= nst && !mbar_wait(&empty[s], ((c / nst) - 1) & 1)) {
         atomicExch(a.err, 4);
         break;
       }
@@ -221,26 +247,31 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
       const uint32_t fb = smem_u32(&full[s]);
       mbar_expect_tx(&full[s], tx_bytes);
       const int kc = (int)(k_begin + (int64_t)c * 64);
-      tma_load_3d(st, &map_hi, kc, rb * TM_BM, zc, fb);
-      for (int q = 0; q < nbox; ++q) tma_load_3d(st + TM_TILE_A + q * TM_BOX * 128, &map_hi, kc, nb * TM_BN + q * TM_BOX, zc, fb);
+      const void* bh = blk.strip ? (const void*)&smap_hi : (const void*)&map_hi;
+      const void* bl = blk.strip ? (const void*)&smap_lo : (const void*)&map_lo;
+      tma_load_3d(st, &map_hi, kc, blk.arow, zc, fb);
+      for (int q = 0; q < nbox; ++q) tma_load_3d(st + TM_TILE_A + q * TM_BOX * 128, bh, kc, blk.brow + q * TM_BOX, zc, fb);
       if (split) {
-        const uint32_t lo = st + TM_TILE_A + TM_TILE_B;
-        tma_load_3d(lo, &map_lo, kc, rb * TM_BM, zc, fb);
-        for (int q = 0; q < nbox; ++q) tma_load_3d(lo + TM_TILE_A + q * TM_BOX * 128, &map_lo, kc, nb * TM_BN + q * TM_BOX, zc, fb);
+        const uint32_t lo = st + TM_TILE_A + b_region;
+        tma_load_3d(lo, &map_lo, kc, blk.arow, zc, fb);
+        for (int q = 0; q < nbox; ++q) tma_load_3d(lo + TM_TILE_A + q * TM_BOX * 128, bl, kc, blk.brow + q * TM_BOX, zc, fb);
       }
     }
+    // the last loads have landed before the CTA may exit (at once unless a
+    // wait above gave up with copies in flight)
+    for (int q = c > nst ? c - nst : 0; q < c; ++q) mbar_wait(&full[q % nst], (q / nst) & 1);
   } else if (warp == 1 && lane == 0) {
     // ------------------------------------------------------------ MMA issuer
     const uint32_t idesc = umma_idesc_bf16(npad);
     for (int c = 0; c < nch; ++c) {
-      const int s = c % TM_STAGES;
-      if (!mbar_wait(&full[s], (c / TM_STAGES) & 1)) {
+      const int s = c % nst;
+      if (!mbar_wait(&full[s], (c / nst) & 1)) {
         atomicExch(a.err, 5);
         break;
       }
       tc_fence_after();
       const uint32_t st = sbase + s * stage_bytes;
-      const uint32_t ahi = st, bhi = st + TM_TILE_A, alo = st + TM_TILE_A + TM_TILE_B, blo = alo + TM_TILE_A;
+      const uint32_t ahi = st, bhi = st + TM_TILE_A, alo = st + TM_TILE_A + b_region, blo = alo + TM_TILE_A;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const uint32_t kb = k * 32;
@@ -262,7 +293,7 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
   __syncwarp();
   tc_fence_after();
   if (!ok && lane == 0) atomicExch(a.err, 6);
-  const int i = rb * TM_BM + warp * 32 + lane;
+  const int i = blk.arow + warp * 32 + lane;
   const uint32_t lane_addr = taddr + ((uint32_t)(warp * 32) << 16);
   for (int cc = 0; cc < npad; cc += 16) {
     float v[16];
@@ -270,8 +301,10 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
     if (!a.cplx) {
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
-        const int j = nb * TM_BN + cc + q;
-        if (ok && i < N && j <= i && (cc + q) < ncols) out[pk(i, j, N)] = v[q];
+        const int j = blk.brow + cc + q;
+        if (!ok || i >= N || (cc + q) >= ncols) continue;
+        if (!blk.strip && j <= i) out[pk(i, j, N)] = v[q];
+        if (blk.strip && j >= i) out[pk(j, i, N)] = v[q];  // G[i][j] = G[j][i], stored as the lower (j, i)
       }
     } else {
       float vp[16];
@@ -282,8 +315,11 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
         cf* oc = reinterpret_cast<cf*>(out);
 #pragma unroll
         for (int q = 0; q < 16; q += 2) {
-          const int jc = (nb * TM_BN + cc + q) >> 1;
-          if (ok && ic < n && jc <= ic && (cc + q) < ncols) oc[pk(ic, jc, n)] = cf{v[q] + vp[q + 1], v[q + 1] - vp[q]};
+          const int jc = (blk.brow + cc + q) >> 1;
+          if (!ok || ic >= n || (cc + q) >= ncols) continue;
+          if (!blk.strip && jc <= ic) oc[pk(ic, jc, n)] = cf{v[q] + vp[q + 1], v[q + 1] - vp[q]};
+          // strip: the lower entry (jc, ic) is the conjugate of (ic, jc)
+          if (blk.strip && jc >= ic) oc[pk(jc, ic, n)] = cf{v[q] + vp[q + 1], vp[q] - v[q + 1]};
         }
       }
     }
@@ -320,14 +356,19 @@ cudaError_t get_encode(EncodeFn* fn) {
   return cudaSuccess;
 }
 
-// 3D bf16 map: (K = kp [contiguous], rows = N, depth), box 64 x 128 x 1, 128-byte swizzle.
-cudaError_t make_map(CUtensorMap* m, const void* base, int64_t kp, int N, int64_t depth) {
+}  // namespace
+
+// 3D bf16 map over [depth][rows][inner] (inner contiguous, a multiple of 64):
+// box 64 x 128 x 1, 128-byte swizzle (the K-major operand layout of tcgen05).
+// Rows past `rows` read as zeros.
+cudaError_t make_bf16_map(CUtensorMap* m, const void* base, int64_t inner, int64_t rows, int64_t depth,
+                          int box_rows) {
   EncodeFn enc;
   cudaError_t e = get_encode(&enc);
   if (e != cudaSuccess) return e;
-  cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)N, (cuuint64_t)depth};
-  cuuint64_t strides[2] = {(cuuint64_t)kp * 2, (cuuint64_t)kp * 2 * N};
-  cuuint32_t box[3] = {64, TM_BOX, 1};
+  cuuint64_t dims[3] = {(cuuint64_t)inner, (cuuint64_t)rows, (cuuint64_t)depth};
+  cuuint64_t strides[2] = {(cuuint64_t)inner * 2, (cuuint64_t)inner * 2 * rows};
+  cuuint32_t box[3] = {64, (cuuint32_t)box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -335,49 +376,76 @@ cudaError_t make_map(CUtensorMap* m, const void* base, int64_t kp, int N, int64_
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-int tm_blocks(int N) {
-  int t = 0;
-  for (int rb = 0; rb * TM_BM < N; ++rb) {
-    const int lim = (rb + 1) * TM_BM < N ? (rb + 1) * TM_BM : N;
-    t += (lim + TM_BN - 1) / TM_BN;
-  }
-  return t;
+namespace {
+size_t tm_smem(int split) {
+  return 1024 + TM_STAGES * (size_t)(split == 3 ? 2 : 1) * (TM_TILE_A + TM_TILE_B) + (2 * TM_MAX_STAGES + 1) * 8 + 16;
 }
-
-size_t tm_smem(int split) { return 1024 + TM_STAGES * (size_t)(split == 3 ? 2 : 1) * (TM_TILE_A + TM_TILE_B) + 64; }
 }  // namespace
 
-size_t packed_bytes_per_patch(int n, bool cplx, int M) {
-  const int N = cplx ? 2 * n : n;
-  return (size_t)2 * 2 * N * pack_k(M);  // hi + lo bf16
+PackedLayout packed_layout(int n, bool cplx, int M, bool synth_tc, int count) {
+  PackedLayout L{};
+  L.N = cplx ? 2 * n : n;
+  L.kp = pack_k(M);
+  L.kn = pack_k(L.N);
+  L.synth_tc = synth_tc;
+  const int64_t gram_el = (int64_t)L.N * L.kp, rows_el = L.kp * L.kn, coef_el = (int64_t)L.N * L.kn;
+  L.hi = 0;
+  L.lo = L.hi + count * gram_el;
+  L.rows_hi = L.lo + count * gram_el;
+  L.rows_lo = L.rows_hi + (synth_tc ? count * rows_el : 0);
+  L.coef_hi = L.rows_lo + (synth_tc ? count * rows_el : 0);
+  L.coef_lo = L.coef_hi + (synth_tc ? count * coef_el : 0);
+  L.total = L.coef_lo + (synth_tc ? count * coef_el : 0);
+  return L;
+}
+
+size_t packed_bytes_per_patch(int n, bool cplx, int M, bool synth_tc) {
+  return (size_t)packed_layout(n, cplx, M, synth_tc, 1).total * sizeof(__nv_bfloat16);
 }
 
 cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const PatchWork& w, void* packed,
-                               cudaStream_t s) {
-  const int N = cplx ? 2 * g.cols : g.cols;
-  const int64_t kp = pack_k(g.rows);
-  __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(packed);
-  __nv_bfloat16* lo = hi + (int64_t)w.count * N * kp;
+                               cudaStream_t s, bool synth_tc) {
+  const PackedLayout L = packed_layout(g.cols, cplx, g.rows, synth_tc, w.count);
+  const int N = L.N;
+  const int64_t kp = L.kp;
+  __nv_bfloat16* base = reinterpret_cast<__nv_bfloat16*>(packed);
+  __nv_bfloat16* hi = base + L.hi;
+  __nv_bfloat16* lo = base + L.lo;
+  __nv_bfloat16* rhi = synth_tc ? base + L.rows_hi : nullptr;
+  __nv_bfloat16* rlo = synth_tc ? base + L.rows_lo : nullptr;
   // K segments per column tile: enough CTAs for about eight waves of 8 per SM
   const int64_t ktiles = kp / PK_R, ctiles = (N + PK_C - 1) / PK_C;
   const int ks = (int)std::min<int64_t>(ktiles, std::max<int64_t>(1, (148 * 8 * 8) / ((int64_t)w.count * ctiles)));
-  if ((int64_t)w.count * ctiles * ks > INT32_MAX || (int64_t)w.count * tm_blocks(N) > INT32_MAX)
+  // strips when N has whole 128-row blocks and a remainder
+  const int nmain = (N >= TM_BM && N % TM_BM != 0) ? N / TM_BM * TM_BM : N;
+  const int sbox = nmain < N ? ((N - nmain + 15) & ~15) : 0;
+  if ((int64_t)w.count * ctiles * ks > INT32_MAX || (int64_t)w.count * tm_blocks(N, nmain) > INT32_MAX)
     return cudaErrorInvalidConfiguration;
   const unsigned pg = (unsigned)(w.count * ctiles * ks);
   PD_TIMED("pack", s,
-           k_pack_patches<<<pg, 256, 0, s>>>(g, (const float*)in, N, cplx ? 1 : 0, w.mean, w.list, hi, lo, kp, ks));
+           k_pack_patches<<<pg, 256, 0, s>>>(g, (const float*)in, N, cplx ? 1 : 0, w.mean, w.list, hi, lo, kp, ks,
+                                             rhi, rlo, L.kn));
   CUtensorMap mh, ml;
-  cudaError_t e = make_map(&mh, hi, kp, N, w.count);
+  cudaError_t e = make_bf16_map(&mh, hi, kp, N, w.count);
   if (e != cudaSuccess) return e;
-  e = make_map(&ml, lo, kp, N, w.count);
+  e = make_bf16_map(&ml, lo, kp, N, w.count);
   if (e != cudaSuccess) return e;
+  CUtensorMap sh = mh, sl = ml;  // the strip's narrow B boxes
+  if (sbox) {
+    e = make_bf16_map(&sh, hi, kp, N, w.count, sbox);
+    if (e != cudaSuccess) return e;
+    e = make_bf16_map(&sl, lo, kp, N, w.count, sbox);
+    if (e != cudaSuccess) return e;
+  }
   TmaArgs a{};
   a.N = N;
   a.n_out = g.cols;
   a.cplx = cplx ? 1 : 0;
   a.split = 3;
   a.kp = kp;
-  a.nblk = tm_blocks(N);
+  a.nmain = nmain;
+  a.sbox = sbox;
+  a.nblk = tm_blocks(N, nmain);
   a.out = w.gram;
   a.out_stride = w.gram_stride;
   a.err = w.err;
@@ -385,7 +453,7 @@ cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const Pa
   e = cudaFuncSetAttribute(k_gram_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const unsigned grid = (unsigned)(w.count * a.nblk);
-  PD_TIMED("gram_tc", s, k_gram_tma<<<grid, TM_THREADS, smem, s>>>(mh, ml, a));
+  PD_TIMED("gram_tc", s, k_gram_tma<<<grid, TM_THREADS, smem, s>>>(mh, ml, sh, sl, a));
   return cudaGetLastError();
 }
 

@@ -1,6 +1,7 @@
 // Launchers shared between the kernel translation units and the C ABI layer.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -146,9 +147,26 @@ cudaError_t launch_backward(const Geo& g, const float* in, const float* gout, co
                             const PatchWork& w, const BwdWork& b, cudaStream_t s);
 
 // pd_gram_tma.cu (pack + TMA-fed tcgen05)
-size_t packed_bytes_per_patch(int n, bool cplx, int M);
+// The mixed path's packed operands of a chunk, in bf16 elements from
+// PatchWork::packed: the Gram's column-major hi / lo [count][N][kp] and, for the
+// tensor-core synthesis, the row-major copy [count][kp][kn] and the synthesis
+// matrix [count][N][kn] (hi / lo each). N real columns, kp = rows rounded up to
+// 64, kn = N rounded up to 64.
+struct PackedLayout {
+  int N;
+  int64_t kp, kn;
+  bool synth_tc;
+  int64_t hi, lo, rows_hi, rows_lo, coef_hi, coef_lo, total;
+};
+PackedLayout packed_layout(int n, bool cplx, int M, bool synth_tc, int count);
+size_t packed_bytes_per_patch(int n, bool cplx, int M, bool synth_tc);
+cudaError_t make_bf16_map(CUtensorMap* m, const void* base, int64_t inner, int64_t rows, int64_t depth,
+                          int box_rows = 128);
 cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const PatchWork& w, void* packed,
-                               cudaStream_t s);
+                               cudaStream_t s, bool synth_tc = false);
+// pd_synth_tc.cu: the tensor-core synthesis (mixed path, weighted / average
+// recombination) from the packed row-major operands launch_gram_packed wrote
+cudaError_t launch_synth_tc(const Geo& g, bool cplx, const PatchWork& w, const SynthArgs& a, cudaStream_t s);
 
 // pd_mc.cu
 // Bartlett-sampled Wishart Grams: n_iter packed d x d Grams distributed as G^T G

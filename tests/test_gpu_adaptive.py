@@ -82,6 +82,22 @@ def test_adaptive_rank_deficient_patches(method, gamma0):
     _check(x, call, "fp32", f"rank-deficient {method}")
 
 
+@pytest.mark.parametrize("cplx,frames,recombination", [(True, 200, "weighted"), (False, 120, "average"),
+                                                        (True, 72, "average"), (False, 300, "weighted")])
+def test_adaptive_mixed_tensor_core_synthesis(cplx, frames, recombination):
+    """The mixed path synthesises adaptive patches on the tensor cores: 11^3-voxel
+    patches (five 256-voxel tiles and a partial one) and frame counts whose real
+    widths (2 x 200, 120, 2 x 72, 300) leave partial 128-column and 64-wide K
+    tiles. Held to the FP64 oracle like the fixtures."""
+    from patch_denoising_b200.synthetic import lowrank_volume
+
+    x, _ = lowrank_volume((17, 17, 11, frames), 5, amplitude=25.0, noise=2.0, complex_valued=cplx, seed=91)
+    x = x.astype(np.complex64 if cplx else np.float32)
+    call = dict(method="adaptive", patch_shape=11, patch_overlap=5, recombination=recombination,
+                adaptive_method="sure", noise_std=2.0, nbsim=100, gamma0=[1.0, 2.0], tau0=None)
+    _check(x, call, "mixed", f"tensor-core synthesis c={cplx} T={frames}")
+
+
 def _check(x, call, precision, name):
     np.random.seed(11)
     (out, weights, _, rank_map), den = _ours(x, call, precision)

@@ -64,6 +64,15 @@ def test_streamed_host_volume_matches_device_path(kind, monkeypatch):
     cdt = np.complex128 if np.iscomplexobj(out_d) else np.float64
     assert rel_l2(out_h[ok].astype(cdt), out_d[ok].astype(cdt)) <= 1e-6
     assert rel_l2(w_h.astype(np.float64), w_d.astype(np.float64)) <= 1e-6
+    # the weights come back as a full, writable array even where only their
+    # spatial part crossed PCIe (patches spanning every frame)
+    assert w_h.flags.writeable and w_h.strides[-1] != 0
+    spans_all = kind != "mppca_time_tiled"
+    frames = x.shape[-1] if spans_all else 1
+    nm_frames = 1 if kind == "optimal_center" else frames  # "center": the full noise map
+    sent = out_h.nbytes + w_h.nbytes // frames + nm_h.nbytes // nm_frames + rm_h.nbytes // frames
+    assert _engine.LAST_TRANSFER["h2d"] == x.nbytes
+    assert _engine.LAST_TRANSFER["d2h"] == sent
     fin = np.isfinite(nm_d)
     np.testing.assert_array_equal(fin, np.isfinite(nm_h))
     if fin.any():
