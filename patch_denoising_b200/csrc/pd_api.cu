@@ -82,6 +82,7 @@ PatchWork carve_work(void* ws, int count, int n, bool cplx, size_t* used, size_t
   Carver c(ws);
   PatchWork w{};
   w.err = c.take<int>(1);  // always at offset 0 of the workspace
+  w.ctr = c.take<int>(1);  // tile counter of the persistent tensor-core kernels
   w.count = count;
   w.n_stride = n;
   w.packed = packed_per_patch ? (void*)c.take<uint8_t>(packed_per_patch * count) : nullptr;

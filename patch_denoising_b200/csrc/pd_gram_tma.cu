@@ -6,16 +6,17 @@
 //   rounded up to 64, zero padded), x = hi + lo to about 16 bits. Reads are
 //   coalesced along frames, writes along voxels through a shared-memory
 //   transpose; the kernel is memory bound and runs at full occupancy.
-// k_gram_tma: CTA = (patch, 128 x <=256 block of the lower Gram). When N is
+// k_gram_tma: tiles = (patch, 128 x <=256 block of the lower Gram). When N is
 //   not a multiple of 128 (N = 400 for 200 complex frames), the last, partial
 //   128-row block would compute mostly padding: its rows are produced instead
 //   as a strip of columns, G[0:N, Nmain:N] (Nmain = N rounded down to 128), by
 //   symmetry, from a narrow B box (the remainder rows only).
-//   One thread issues cp.async.bulk.tensor loads (128-byte swizzle, the
-//   canonical K-major layout of tcgen05) into a 2-stage ring guarded by
-//   mbarriers with transaction counts; one thread issues tcgen05.mma with the
-//   accumulator in TMEM (hi*hi + hi*lo + lo*hi);
-//   four warps read TMEM and write the packed Gram (complex via 2x2 blocks).
+//   Persistent (one CTA per SM over the tiles) and warp-specialised: one
+//   thread issues cp.async.bulk.tensor loads (128-byte swizzle, the canonical
+//   K-major layout of tcgen05) into a 2-stage ring guarded by mbarriers with
+//   transaction counts; one thread issues tcgen05.mma (hi*hi + hi*lo + lo*hi)
+//   into one of two TMEM accumulators; four warps read the other accumulator
+//   and write the packed Gram (complex via 2x2 blocks).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -35,9 +36,9 @@ constexpr int PK_C = 64;  // columns per pack tile
 constexpr int TM_BM = 128;
 constexpr int TM_BN = 256;
 constexpr int TM_BOX = 128;  // rows per TMA box
-constexpr int TM_STAGES = 2;      // stages of a full-width block
-constexpr int TM_MAX_STAGES = 6;  // a strip block's narrow stages fit more in the same area
-constexpr int TM_THREADS = 128;
+constexpr int TM_STAGES = 2;  // operand stages (hi and lo of A and B each)
+constexpr int TM_TQ = 4;      // claimed tile indices in flight between the roles
+constexpr int TM_THREADS = 192;  // warps 0-3 epilogue, 4 TMA, 5 MMA
 constexpr uint32_t TM_TILE_A = TM_BM * 128;
 constexpr uint32_t TM_TILE_B = TM_BN * 128;
 
@@ -145,9 +146,10 @@ struct TmaArgs {
   int sbox;    // rows of the strip's B box (the remainder rounded up to 16), 0 without strips
   int n_out;   // output order (N or N/2 for complex)
   int cplx;
-  int split;   // 3: hi/lo, 1: hi only
   int64_t kp;  // packed K extent
-  int nblk;    // Gram blocks per patch (grid flattened with the block fastest)
+  int nblk;    // Gram blocks per patch
+  int count;   // patches
+  int* ctr;    // next unclaimed tile (zero at launch)
   float* out;
   int64_t out_stride;
   int* err;
@@ -178,6 +180,41 @@ __host__ __device__ inline int tm_blocks(int N, int nmain) {
   return t;
 }
 
+// Persistent and warp-specialised: one CTA per SM walks the (patch, block)
+// tiles. Warp 4 issues the TMA loads into a 2-stage ring (running ahead into
+// the next tile), warp 5 the MMAs into one of two 256-column TMEM accumulators,
+// warps 0-3 write the other accumulator's block into the packed Gram, so a
+// tile's epilogue overlaps the next tile's loads and MMAs.
+__device__ __forceinline__ void tm_store(const TmaArgs& a, const TmBlock& blk, float* out, int i, int cc,
+                                         const float v[16]) {
+  const int N = a.N;
+  if (!a.cplx) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int j = blk.brow + cc + q;
+      if (i >= N || (cc + q) >= blk.ncols) continue;
+      if (!blk.strip && j <= i) out[pk(i, j, N)] = v[q];
+      if (blk.strip && j >= i) out[pk(j, i, N)] = v[q];  // G[i][j] = G[j][i], stored as the lower (j, i)
+    }
+  } else {
+    float vp[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) vp[q] = __shfl_xor_sync(0xffffffffu, v[q], 1);
+    if ((i & 1) == 0) {
+      const int ic = i >> 1, n = a.n_out;
+      cf* oc = reinterpret_cast<cf*>(out);
+#pragma unroll
+      for (int q = 0; q < 16; q += 2) {
+        const int jc = (blk.brow + cc + q) >> 1;
+        if (ic >= n || (cc + q) >= blk.ncols) continue;
+        if (!blk.strip && jc <= ic) oc[pk(ic, jc, n)] = cf{v[q] + vp[q + 1], v[q + 1] - vp[q]};
+        // strip: the lower entry (jc, ic) is the conjugate of (ic, jc)
+        if (blk.strip && jc >= ic) oc[pk(jc, ic, n)] = cf{v[q] + vp[q + 1], vp[q] - v[q + 1]};
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constant__ CUtensorMap map_hi,
                                                              const __grid_constant__ CUtensorMap map_lo,
                                                              const __grid_constant__ CUtensorMap smap_hi,
@@ -186,149 +223,204 @@ __global__ void __launch_bounds__(TM_THREADS, 1) k_gram_tma(const __grid_constan
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = a.N;
-  const bool split = a.split == 3;
-  const uint32_t stage_area = TM_STAGES * (split ? 2u : 1u) * (TM_TILE_A + TM_TILE_B);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + stage_area);
-  uint64_t* full = bars;
-  uint64_t* empty = bars + TM_MAX_STAGES;
-  uint64_t* done = bars + 2 * TM_MAX_STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
-
-  // The Gram blocks that read the same operand rows (of one patch) are
-  // consecutive in the flattened grid (patch, block), so they share those rows in L2.
-  const int bidx = (int)(blockIdx.x % (unsigned)a.nblk);
-  const int pidx = (int)(blockIdx.x / (unsigned)a.nblk);
-  const TmBlock blk = tm_block_of(bidx, N, a.nmain);
-  const int ncols = blk.ncols;
-  const int npad = (ncols + 15) & ~15;
-  const int nbox = blk.strip ? 1 : (npad + TM_BOX - 1) / TM_BOX;  // B boxes of 128 rows (strip: one narrow box)
-  const uint32_t bbox_bytes = blk.strip ? (uint32_t)a.sbox * 128u : (uint32_t)TM_BOX * 128u;
-  // a stage holds A and B (hi, then lo); a strip's B is narrow, so its ring is
-  // deeper (its MMAs are short and its loads must be in flight to hide latency)
-  const uint32_t b_region = blk.strip ? bbox_bytes : TM_TILE_B;
-  const uint32_t stage_bytes = (split ? 2u : 1u) * (TM_TILE_A + b_region);
-  const int nst = min(TM_MAX_STAGES, (int)(stage_area / stage_bytes));
-  uint32_t tcols = 32;
-  while (tcols < (uint32_t)npad) tcols <<= 1;
-
-  const int64_t k_begin = 0, k_end = a.kp;
-  const int zc = pidx;  // third tensor-map coordinate: the patch
-  float* out = a.out + (int64_t)pidx * a.out_stride;
-  const int nch = (int)((k_end - k_begin + 63) / 64);
-  const uint32_t tx_bytes = (split ? 2u : 1u) * (TM_TILE_A + (uint32_t)nbox * bbox_bytes);
+  constexpr uint32_t STAGE = 2 * (TM_TILE_A + TM_TILE_B);  // hi, then lo
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + TM_STAGES * STAGE);
+  uint64_t* full = bars;                   // [TM_STAGES]
+  uint64_t* empty = bars + TM_STAGES;      // [TM_STAGES]
+  uint64_t* tfull = bars + 2 * TM_STAGES;  // [2]
+  uint64_t* tempty = tfull + 2;            // [2]
+  uint64_t* done = tempty + 2;
+  uint64_t* qfull = done + 1;      // [TM_TQ] a claimed tile index is in the queue
+  uint64_t* qempty = qfull + TM_TQ;  // [TM_TQ] its slot is free again
+  volatile int* tileq = reinterpret_cast<volatile int*>(qempty + TM_TQ);  // [TM_TQ]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(const_cast<int*>(tileq) + TM_TQ);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);  // any role gave up
+  volatile int* epi_abort = abort_flag + 1;  // written and read by the epilogue warps only
+  volatile int* tileq_epi = abort_flag + 2;  // the epilogue's current tile (its warp 0 writes it)
 
   if (tid == 0) {
-    for (int s = 0; s < nst; ++s) {
+    for (int s = 0; s < TM_STAGES; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
+    }
     mbar_init(done, 1);
+    for (int q = 0; q < TM_TQ; ++q) {
+      mbar_init(&qfull[q], 1);
+      mbar_init(&qempty[q], 1);
+    }
+    *abort_flag = 0;
+    *epi_abort = 0;
     mbar_fence_init();
   }
-  if (warp == 1) {
-    tmem_alloc(tmem_slot, tcols);
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, 512);  // two 256-column accumulators
     tc_fence_before();
   }
   __syncthreads();
   tc_fence_after();
   const uint32_t taddr = *tmem_slot;
   const uint32_t sbase = smem_u32(sm);
+  const int nch = (int)((a.kp + 63) / 64);
+  const int tiles = a.count * a.nblk;
+  // Tiles are claimed in (patch, block) order from a global counter (a CTA
+  // that starts late, its SM held by another stream's kernel, takes fewer):
+  // a patch's blocks, and its overlapping neighbours', read the same operand
+  // rows close together in time (L2). The producer passes each claimed index
+  // to the MMA and epilogue warps through a small shared-memory queue; -1 ends.
+  // Returns the i-th claimed tile for a consumer role (-1: none left or a wait gave up).
+  auto next_tile = [&](int i) -> int {
+    const int q = i % TM_TQ;
+    if (!mbar_wait(&qfull[q], (i / TM_TQ) & 1)) return -1;
+    return tileq[q];
+  };
 
-  if (warp == 0 && lane == 0) {
+  if (warp == 4) {
     // ------------------------------------------------------------ TMA producer
-    int c = 0;
-    for (; c < nch; ++c) {
-      const int s = c % nst;
-      if (c >= nst && !mbar_wait(&empty[s], ((c / nst) - 1) & 1)) {
-        atomicExch(a.err, 4);
-        break;
+    if (lane == 0) {
+      int c = 0;
+      for (int i = 0;; ++i) {
+        const int q = i % TM_TQ;
+        if (i >= TM_TQ && !mbar_wait(&qempty[q], ((i / TM_TQ) - 1) & 1)) {
+          atomicExch(a.err, 4);
+          *abort_flag = 1;
+        }
+        int t = *abort_flag ? -1 : atomicAdd(a.ctr, 1);
+        if (t >= tiles) t = -1;
+        tileq[q] = t;
+        mbar_arrive(&qfull[q]);
+        if (t < 0) break;
+        const int p = t / a.nblk;
+        const TmBlock blk = tm_block_of(t - p * a.nblk, N, a.nmain);
+        const int npad = (blk.ncols + 15) & ~15;
+        const int nbox = blk.strip ? 1 : (npad + TM_BOX - 1) / TM_BOX;
+        const uint32_t bbox = blk.strip ? (uint32_t)a.sbox * 128u : (uint32_t)TM_BOX * 128u;
+        const uint32_t tx = 2u * (TM_TILE_A + (uint32_t)nbox * bbox);
+        const void* bh = blk.strip ? (const void*)&smap_hi : (const void*)&map_hi;
+        const void* bl = blk.strip ? (const void*)&smap_lo : (const void*)&map_lo;
+        bool ok = true;
+        for (int k = 0; k < nch; ++k, ++c) {
+          const int s = c % TM_STAGES;
+          if (c >= TM_STAGES && !mbar_wait(&empty[s], ((c / TM_STAGES) - 1) & 1)) {
+            atomicExch(a.err, 4);
+            *abort_flag = 1;
+            ok = false;
+            break;
+          }
+          const uint32_t st = sbase + s * STAGE;
+          const uint32_t fb = smem_u32(&full[s]);
+          mbar_expect_tx(&full[s], tx);
+          const int kc = k * 64;
+          tma_load_3d(st, &map_hi, kc, blk.arow, p, fb);
+          for (int q = 0; q < nbox; ++q) tma_load_3d(st + TM_TILE_A + q * TM_BOX * 128, bh, kc, blk.brow + q * TM_BOX, p, fb);
+          const uint32_t lo = st + TM_TILE_A + TM_TILE_B;
+          tma_load_3d(lo, &map_lo, kc, blk.arow, p, fb);
+          for (int q = 0; q < nbox; ++q) tma_load_3d(lo + TM_TILE_A + q * TM_BOX * 128, bl, kc, blk.brow + q * TM_BOX, p, fb);
+        }
+        if (!ok) break;
       }
-      const uint32_t st = sbase + s * stage_bytes;
-      const uint32_t fb = smem_u32(&full[s]);
-      mbar_expect_tx(&full[s], tx_bytes);
-      const int kc = (int)(k_begin + (int64_t)c * 64);
-      const void* bh = blk.strip ? (const void*)&smap_hi : (const void*)&map_hi;
-      const void* bl = blk.strip ? (const void*)&smap_lo : (const void*)&map_lo;
-      tma_load_3d(st, &map_hi, kc, blk.arow, zc, fb);
-      for (int q = 0; q < nbox; ++q) tma_load_3d(st + TM_TILE_A + q * TM_BOX * 128, bh, kc, blk.brow + q * TM_BOX, zc, fb);
-      if (split) {
-        const uint32_t lo = st + TM_TILE_A + b_region;
-        tma_load_3d(lo, &map_lo, kc, blk.arow, zc, fb);
-        for (int q = 0; q < nbox; ++q) tma_load_3d(lo + TM_TILE_A + q * TM_BOX * 128, bl, kc, blk.brow + q * TM_BOX, zc, fb);
-      }
+      // the last loads have landed before the CTA may exit (at once unless a
+      // wait above gave up with copies in flight)
+      for (int q = c > TM_STAGES ? c - TM_STAGES : 0; q < c; ++q) mbar_wait(&full[q % TM_STAGES], (q / TM_STAGES) & 1);
     }
-    // the last loads have landed before the CTA may exit (at once unless a
-    // wait above gave up with copies in flight)
-    for (int q = c > nst ? c - nst : 0; q < c; ++q) mbar_wait(&full[q % nst], (q / nst) & 1);
-  } else if (warp == 1 && lane == 0) {
+  } else if (warp == 5) {
     // ------------------------------------------------------------ MMA issuer
-    const uint32_t idesc = umma_idesc_bf16(npad);
-    for (int c = 0; c < nch; ++c) {
-      const int s = c % nst;
-      if (!mbar_wait(&full[s], (c / nst) & 1)) {
-        atomicExch(a.err, 5);
-        break;
-      }
-      tc_fence_after();
-      const uint32_t st = sbase + s * stage_bytes;
-      const uint32_t ahi = st, bhi = st + TM_TILE_A, alo = st + TM_TILE_A + b_region, blo = alo + TM_TILE_A;
+    if (lane == 0) {
+      int c = 0;
+      for (int i = 0;; ++i) {
+        const int t = *abort_flag ? -1 : next_tile(i);
+        if (t < 0) break;
+        const int p = t / a.nblk;
+        const TmBlock blk = tm_block_of(t - p * a.nblk, N, a.nmain);
+        const int npad = (blk.ncols + 15) & ~15;
+        const uint32_t idesc = umma_idesc_bf16(npad);
+        const int b = i & 1;
+        if (i >= 2 && !mbar_wait(&tempty[b], ((i >> 1) - 1) & 1)) {
+          atomicExch(a.err, 5);
+          *abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc = taddr + (uint32_t)(b * TM_BN);
+        bool ok = true;
+        for (int k = 0; k < nch; ++k, ++c) {
+          const int s = c % TM_STAGES;
+          if (!mbar_wait(&full[s], (c / TM_STAGES) & 1)) {
+            atomicExch(a.err, 5);
+            *abort_flag = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = sbase + s * STAGE;
+          const uint32_t ahi = st, bhi = st + TM_TILE_A, alo = st + TM_TILE_A + TM_TILE_B, blo = alo + TM_TILE_A;
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const uint32_t kb = k * 32;
-        const uint64_t da = umma_desc_sw128(ahi + kb), db = umma_desc_sw128(bhi + kb);
-        umma_bf16(taddr, da, db, idesc, (c | k) != 0 ? 1u : 0u);
-        if (split) {
-          umma_bf16(taddr, da, umma_desc_sw128(blo + kb), idesc, 1u);
-          umma_bf16(taddr, umma_desc_sw128(alo + kb), db, idesc, 1u);
+          for (int kk = 0; kk < 4; ++kk) {
+            const uint32_t kb = kk * 32;
+            const uint64_t da = umma_desc_sw128(ahi + kb), db = umma_desc_sw128(bhi + kb);
+            umma_bf16(acc, da, db, idesc, (k | kk) != 0 ? 1u : 0u);
+            umma_bf16(acc, da, umma_desc_sw128(blo + kb), idesc, 1u);
+            umma_bf16(acc, umma_desc_sw128(alo + kb), db, idesc, 1u);
+          }
+          umma_commit(&empty[s]);
+        }
+        if (!ok) break;
+        umma_commit(&tfull[b]);
+      }
+      umma_commit(done);
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue (warps 0-3)
+    for (int i = 0;; ++i) {
+      // warp 0 takes the tile index and the tile's accumulator; the others follow at the barrier
+      int t = -1;
+      if (warp == 0) {
+        t = *abort_flag ? -1 : next_tile(i);
+        if (lane == 0) {
+          tileq_epi[0] = t;
+          if (t >= 0 && !mbar_wait(&tfull[i & 1], (i >> 1) & 1)) {
+            atomicExch(a.err, 6);
+            *epi_abort = 1;
+          }
+          if (t >= 0) mbar_arrive(&qempty[i % TM_TQ]);  // the index has been read by every role
         }
       }
-      umma_commit(&empty[s]);
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      t = tileq_epi[0];
+      if (t < 0 || *epi_abort) break;  // the same decision in all four warps
+      const int p = t / a.nblk;
+      const TmBlock blk = tm_block_of(t - p * a.nblk, N, a.nmain);
+      const int npad = (blk.ncols + 15) & ~15;
+      const int b = i & 1;
+      tc_fence_after();
+      float* out = a.out + (int64_t)p * a.out_stride;
+      const int row = blk.arow + warp * 32 + lane;
+      const uint32_t lane_addr = taddr + (uint32_t)(b * TM_BN) + ((uint32_t)(warp * 32) << 16);
+      for (int cc = 0; cc < npad; cc += 16) {
+        float v[16];
+        tmem_ld16(lane_addr + cc, v);
+        tm_store(a, blk, out, row, cc, v);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);
+      asm volatile("bar.sync 1, 128;" ::: "memory");  // tileq_epi is free for the next tile
     }
-    umma_commit(done);
   }
   __syncwarp();
-
-  // ------------------------------------------------------------ epilogue (4 warps)
-  const bool ok = mbar_wait(done, 0);
-  __syncwarp();
-  tc_fence_after();
-  if (!ok && lane == 0) atomicExch(a.err, 6);
-  const int i = blk.arow + warp * 32 + lane;
-  const uint32_t lane_addr = taddr + ((uint32_t)(warp * 32) << 16);
-  for (int cc = 0; cc < npad; cc += 16) {
-    float v[16];
-    tmem_ld16(lane_addr + cc, v);
-    if (!a.cplx) {
-#pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int j = blk.brow + cc + q;
-        if (!ok || i >= N || (cc + q) >= ncols) continue;
-        if (!blk.strip && j <= i) out[pk(i, j, N)] = v[q];
-        if (blk.strip && j >= i) out[pk(j, i, N)] = v[q];  // G[i][j] = G[j][i], stored as the lower (j, i)
-      }
-    } else {
-      float vp[16];
-#pragma unroll
-      for (int q = 0; q < 16; ++q) vp[q] = __shfl_xor_sync(0xffffffffu, v[q], 1);
-      if ((i & 1) == 0) {
-        const int ic = i >> 1, n = a.n_out;
-        cf* oc = reinterpret_cast<cf*>(out);
-#pragma unroll
-        for (int q = 0; q < 16; q += 2) {
-          const int jc = (blk.brow + cc + q) >> 1;
-          if (!ok || ic >= n || (cc + q) >= ncols) continue;
-          if (!blk.strip && jc <= ic) oc[pk(ic, jc, n)] = cf{v[q] + vp[q + 1], v[q + 1] - vp[q]};
-          // strip: the lower entry (jc, ic) is the conjugate of (ic, jc)
-          if (blk.strip && jc >= ic) oc[pk(jc, ic, n)] = cf{v[q] + vp[q + 1], vp[q] - v[q + 1]};
-        }
-      }
-    }
+  // every MMA has completed before TMEM is released
+  if (warp == 0) {
+    const bool ok = mbar_wait(done, 0);
+    if (!ok && lane == 0) atomicExch(a.err, 6);
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 1) {
+  if (warp == 0) {
     tc_fence_after();
-    tmem_dealloc(taddr, tcols);
+    tmem_dealloc(taddr, 512);
   }
 }
 
@@ -377,8 +469,9 @@ cudaError_t make_bf16_map(CUtensorMap* m, const void* base, int64_t inner, int64
 }
 
 namespace {
-size_t tm_smem(int split) {
-  return 1024 + TM_STAGES * (size_t)(split == 3 ? 2 : 1) * (TM_TILE_A + TM_TILE_B) + (2 * TM_MAX_STAGES + 1) * 8 + 16;
+size_t tm_smem() {
+  return 1024 + TM_STAGES * (size_t)2 * (TM_TILE_A + TM_TILE_B) + (2 * TM_STAGES + 5 + 2 * TM_TQ) * 8 +
+         TM_TQ * 4 + 32;
 }
 }  // namespace
 
@@ -441,7 +534,6 @@ cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const Pa
   a.N = N;
   a.n_out = g.cols;
   a.cplx = cplx ? 1 : 0;
-  a.split = 3;
   a.kp = kp;
   a.nmain = nmain;
   a.sbox = sbox;
@@ -449,10 +541,16 @@ cudaError_t launch_gram_packed(const Geo& g, bool cplx, const void* in, const Pa
   a.out = w.gram;
   a.out_stride = w.gram_stride;
   a.err = w.err;
-  const size_t smem = tm_smem(3);
+  const size_t smem = tm_smem();
   e = cudaFuncSetAttribute(k_gram_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  const unsigned grid = (unsigned)(w.count * a.nblk);
+  a.count = w.count;
+  a.ctr = w.ctr;
+  if (cudaError_t ez = cudaMemsetAsync(w.ctr, 0, sizeof(int), s); ez != cudaSuccess) return ez;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned grid = (unsigned)std::min<int64_t>((int64_t)w.count * a.nblk, sms);
   PD_TIMED("gram_tc", s, k_gram_tma<<<grid, TM_THREADS, smem, s>>>(mh, ml, sh, sl, a));
   return cudaGetLastError();
 }

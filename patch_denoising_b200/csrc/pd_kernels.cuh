@@ -71,6 +71,7 @@ struct PatchWork {
   float* noise;         // [count] noise_var (NaN if none)
   double* prior;        // [count] hybrid varest / optimal sigma prior
   int* err;             // device error word (0 = ok)
+  int* ctr;             // tile counter of a persistent kernel (zeroed before each launch)
   void* packed;         // mixed precision: bf16 hi/lo operands of the chunk
   int32_t n_stride;     // frames per patch slot of mean / coef (the largest n of a batch)
   const VolDesc* vols;  // batched call: the volumes (NULL: one volume, the launch's Geo)
