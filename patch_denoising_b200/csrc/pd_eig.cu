@@ -1092,48 +1092,13 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
   }
   __syncthreads();
 
-  // re-orthogonalise inside clusters (descending order; rare)
+  // re-orthogonalise inside clusters (descending order; rare for the low-rank
+  // rules, a whole noise bulk for the adaptive ones)
   {
     const float ortol = 1e-3f * ti.tnorm;
-    int cstart = 0;
-    for (int a = 1; a < act; ++a) {
-      if (alam[a - 1] - alam[a] > ortol) {
-        cstart = a;
-        continue;
-      }
-      float* za = vbase + (int64_t)a * n2;
-      if constexpr (ADAPT) {
-        // Adaptive shrinkage keeps whole noise bulks, one cluster of up to n
-        // vectors: classical Gram-Schmidt against the cluster, twice. The
-        // projections of a pass are independent (a warp per earlier vector),
-        // so a vector costs four barriers instead of three per earlier vector.
-        float* dots = reinterpret_cast<float*>(idx);  // free after the decisions
-        for (int pass = 0; pass < 2; ++pass) {
-          for (int b = cstart + warp; b < a; b += EIG_NW) {
-            const float* zb = vbase + (int64_t)b * n2;
-            float dp = 0.f;
-            for (int i = lane; i < n; i += 32) dp += za[i] * zb[i];
-            dp = warp_sum(dp);
-            if (lane == 0) dots[b - cstart] = dp;
-          }
-          __syncthreads();
-          for (int i = tid; i < n; i += EIG_THREADS) {
-            float v = za[i];
-            for (int b = cstart; b < a; ++b) v -= dots[b - cstart] * vbase[(int64_t)b * n2 + i];
-            za[i] = v;
-          }
-          __syncthreads();
-        }
-      } else {
-        for (int b = cstart; b < a; ++b) {
-          const float* zb = vbase + (int64_t)b * n2;
-          float part = 0.f;
-          for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * zb[i];
-          const float dt = bsum_f(part);
-          for (int i = tid; i < n; i += EIG_THREADS) za[i] -= dt * zb[i];
-          __syncthreads();
-        }
-      }
+    // norm of za, orthogonalised against [cstart, a); a collapsed vector is
+    // replaced by inverse iteration from a pseudo-random start; normalised
+    auto finish = [&](float* za, int a, int cstart) {
       float part = 0.f;
       for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * za[i];
       float nr = sqrtf(bsum_f(part));
@@ -1185,61 +1150,181 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
       const float iv = nr > 0.f ? 1.f / nr : 0.f;
       for (int i = tid; i < n; i += EIG_THREADS) za[i] *= iv;
       __syncthreads();
+    };
+    if constexpr (ADAPT) {
+      // A noise bulk is one cluster of up to n vectors: block classical
+      // Gram-Schmidt, twice. RB vectors at a time are staged in shared memory
+      // and projected against the earlier vectors of their cluster (each
+      // earlier vector is read once per block, a warp per earlier vector for
+      // the dot products), then against each other.
+      constexpr int RB = 8;
+      int* cst = reinterpret_cast<int*>(lam);  // cluster start of each vector (lam is free here)
+      float* blk = reinterpret_cast<float*>(pw);  // [RB][n]; pw (>= 16 n floats) is free after the rule
+      float* dots = blk + RB * n;                 // [RB][act]
+      if (tid == 0) {
+        int c0 = 0;
+        cst[0] = 0;
+        for (int q = 1; q < act; ++q) {
+          if (alam[q - 1] - alam[q] > ortol) c0 = q;
+          cst[q] = c0;
+        }
+      }
+      __syncthreads();
+      for (int a0 = 1; a0 < act; a0 += RB) {
+        const int nb = min(RB, act - a0);
+        const int lo = cst[a0];
+        for (int q = tid; q < nb * n; q += EIG_THREADS) {
+          const int k = q / n, i = q - k * n;
+          blk[k * n + i] = vbase[(int64_t)(a0 + k) * n2 + i];
+        }
+        __syncthreads();
+        for (int pass = 0; pass < 2 && lo < a0; ++pass) {
+          for (int b = lo + warp; b < a0; b += EIG_NW) {
+            const float* zb = vbase + (int64_t)b * n2;
+            float dp[RB];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) dp[k] = 0.f;
+            for (int i = lane; i < n; i += 32) {
+              const float zv = zb[i];
+#pragma unroll
+              for (int k = 0; k < RB; ++k)
+                if (k < nb) dp[k] += zv * blk[k * n + i];
+            }
+#pragma unroll
+            for (int k = 0; k < RB; ++k) {
+              if (k >= nb) break;
+              const float t = warp_sum(dp[k]);
+              if (lane == 0) dots[k * act + b] = b >= cst[a0 + k] ? t : 0.f;
+            }
+          }
+          __syncthreads();
+          for (int i = tid; i < n; i += EIG_THREADS) {
+            float acc[RB];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) acc[k] = 0.f;
+            for (int b = lo; b < a0; ++b) {
+              const float zv = vbase[(int64_t)b * n2 + i];
+#pragma unroll
+              for (int k = 0; k < RB; ++k) acc[k] += dots[k * act + b] * zv;
+            }
+#pragma unroll
+            for (int k = 0; k < RB; ++k)
+              if (k < nb) blk[k * n + i] -= acc[k];
+          }
+          __syncthreads();
+        }
+        // within the block, in order; each vector is final (and back in
+        // global memory) before the next one is projected against it
+        for (int k = 0; k < nb; ++k) {
+          const int a = a0 + k;
+          float* za = vbase + (int64_t)a * n2;
+          if (cst[a] == a) {  // starts a cluster: nothing to project out
+            __syncthreads();
+            continue;
+          }
+          const int j0 = max(cst[a], a0) - a0;
+          for (int pass = 0; pass < 2 && j0 < k; ++pass) {
+            for (int j = j0 + warp; j < k; j += EIG_NW) {
+              float dp = 0.f;
+              for (int i = lane; i < n; i += 32) dp += blk[j * n + i] * blk[k * n + i];
+              dp = warp_sum(dp);
+              if (lane == 0) dots[j] = dp;
+            }
+            __syncthreads();
+            for (int i = tid; i < n; i += EIG_THREADS) {
+              float v = blk[k * n + i];
+              for (int j = j0; j < k; ++j) v -= dots[j] * blk[j * n + i];
+              blk[k * n + i] = v;
+            }
+            __syncthreads();
+          }
+          for (int i = tid; i < n; i += EIG_THREADS) za[i] = blk[k * n + i];
+          __syncthreads();
+          finish(za, a, cst[a]);
+          for (int i = tid; i < n; i += EIG_THREADS) blk[k * n + i] = za[i];
+          __syncthreads();
+        }
+      }
+    } else {
+      int cstart = 0;
+      for (int a = 1; a < act; ++a) {
+        if (alam[a - 1] - alam[a] > ortol) {
+          cstart = a;
+          continue;
+        }
+        float* za = vbase + (int64_t)a * n2;
+        for (int b = cstart; b < a; ++b) {
+          const float* zb = vbase + (int64_t)b * n2;
+          float part = 0.f;
+          for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * zb[i];
+          const float dt = bsum_f(part);
+          for (int i = tid; i < n; i += EIG_THREADS) za[i] -= dt * zb[i];
+          __syncthreads();
+        }
+        finish(za, a, cstart);
+      }
     }
   }
 
-  // back-transform: y = H_0 H_1 ... H_{n-2} z, one warp per vector
-  for (int a = warp; a < act; a += EIG_NW) {
-    float* col = vbase + (int64_t)a * n2;
-    T y[NS];
+  // back-transform: y = H_0 H_1 ... H_{n-2} z. A warp applies each reflector
+  // to VG vectors at once: the reflector column is read once for all of them
+  // and their VG dot products reduce in parallel (whole spectra: act = n).
+  constexpr int VGR = 48 / (NS * (CPLX ? 2 : 1));
+  constexpr int VG = VGR < 1 ? 1 : (VGR > 8 ? 8 : VGR);
+  for (int g0 = warp * VG; g0 < act; g0 += EIG_NW * VG) {
+    T y[VG][NS];
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      const int i = lane + 32 * s;
-      float zv = i < n ? col[i] : 0.f;
-      if constexpr (CPLX) y[s] = cf{zv, 0.f};
-      else y[s] = zv;
+    for (int v = 0; v < VG; ++v) {
+      const float* col = vbase + (int64_t)(g0 + v) * n2;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int i = lane + 32 * s;
+        const float zv = (g0 + v < act && i < n) ? col[i] : 0.f;
+        if constexpr (CPLX) y[v][s] = cf{zv, 0.f};
+        else y[v][s] = zv;
+      }
     }
     for (int j = n - 2; j >= 0; --j) {
       const T tj = tau[j];
       if (abs2(tj) == 0.f) continue;
-      T part = zero<T>();
+      T hv[NS];
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
         const int i = lane + 32 * s;
-        if (i >= j + 1 && i < n) {
-          T v;
-          if (i == j + 1) {
-            if constexpr (CPLX) v = cf{1.f, 0.f};
-            else v = 1.f;
-          } else {
-            v = A[pk(i, j, n)];
-          }
-          part = part + cmulc(v, y[s]);
+        if (i == j + 1) {
+          if constexpr (CPLX) hv[s] = cf{1.f, 0.f};
+          else hv[s] = 1.f;
+        } else {
+          hv[s] = (i > j + 1 && i < n) ? A[pk(i, j, n)] : zero<T>();
         }
       }
-      const T dt = mul(tj, warp_sum(part));
+      T dt[VG];
 #pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        const int i = lane + 32 * s;
-        if (i >= j + 1 && i < n) {
-          T v;
-          if (i == j + 1) {
-            if constexpr (CPLX) v = cf{1.f, 0.f};
-            else v = 1.f;
-          } else {
-            v = A[pk(i, j, n)];
-          }
-          y[s] = y[s] - mul(v, dt);
-        }
+      for (int v = 0; v < VG; ++v) {
+        T part = zero<T>();
+#pragma unroll
+        for (int s = 0; s < NS; ++s) part = part + cmulc(hv[s], y[v][s]);
+        dt[v] = part;
       }
+#pragma unroll
+      for (int v = 0; v < VG; ++v) dt[v] = mul(tj, warp_sum(dt[v]));
+#pragma unroll
+      for (int v = 0; v < VG; ++v)
+#pragma unroll
+        for (int s = 0; s < NS; ++s) y[v][s] = y[v][s] - mul(hv[s], dt[v]);
     }
     __syncwarp();
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      const int i = lane + 32 * s;
-      if (i < n) {
-        if constexpr (CPLX) reinterpret_cast<cf*>(col)[i] = y[s];
-        else col[i] = y[s];
+    for (int v = 0; v < VG; ++v) {
+      if (g0 + v >= act) break;
+      float* col = vbase + (int64_t)(g0 + v) * n2;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < n) {
+          if constexpr (CPLX) reinterpret_cast<cf*>(col)[i] = y[v][s];
+          else col[i] = y[v][s];
+        }
       }
     }
   }
