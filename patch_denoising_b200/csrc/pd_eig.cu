@@ -678,6 +678,39 @@ __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adap
                                            float* alam, float* acoef, double* scratch, double tscale, double M,
                                            double pt, int* s_act) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (ad.mode == PD_ADAPTIVE_QUT && ad.n_gamma >= 1) {
+    // QUT with a fixed gamma: tau = stdest * level is known (lowrank.py:464-475)
+    // and d = s max(1 - (tau / s)^gamma, 0) (lowrank.py:459-461) is nonzero
+    // exactly for s > tau, a prefix of the descending spectrum: only those
+    // eigenvalues are needed (candidates by a Sturm count, as the raw rule)
+    __shared__ int s_c0q;
+    const double tau = sqrt(w.prior[p]) * ad.qut_level;
+    if (tid == 0) s_c0q = sturm_count(d, e2, n, (float)(tau * tau / tscale * (1.0 - CAND_MARGIN)), ti.pivmin);
+    __syncthreads();
+    const int nc = n - s_c0q;
+    for (int i = tid; i < nc; i += EIG_THREADS) idx[i] = s_c0q + i;
+    __syncthreads();
+    cta_eigs(d, e2, n, ti, idx, lam, nc);
+    if (tid == 0) {
+      const double gq = ad.gamma[0], lt = log(tau);
+      int r = 0;
+      for (int i = nc - 1; i >= 0; --i) {
+        const double sv = sqrt(fmax((double)lam[i] * tscale, 0.0));
+        if (!(sv > 0.0)) break;
+        const double dh = sv * np_max0(1.0 - exp(gq * (lt - log(sv))));
+        if (dh == 0.0) break;
+        aidx[r] = idx[i];
+        alam[r] = lam[i];
+        acoef[r] = (float)(dh / sv);
+        ++r;
+      }
+      w.rank[p] = r;
+      w.noise[p] = nanf("");
+      *s_act = r;
+    }
+    __syncthreads();
+    return;
+  }
   // the whole spectrum: singular values s = sqrt(eigenvalue) in numpy.svd's
   // (descending) order, min(M, n) of them
   for (int i = tid; i < n; i += EIG_THREADS) idx[i] = i;
