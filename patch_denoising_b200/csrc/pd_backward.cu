@@ -268,8 +268,11 @@ __global__ void __launch_bounds__(BW_THREADS, 1) k_bwd_small(int n, int M, Patch
 }
 
 // dL/dx += scatter(Xc K1 + Gb K2 + 1 u^T): grid (patch, row block), K1 and K2
-// in shared memory; a warp takes 4 rows at a time, lanes over the frames.
-constexpr int AP_ROWS = 4;
+// in shared memory. A warp takes AP_ROWS rows at a time, staged k-major (row
+// index fastest, so one 16-byte load gives four rows of a frame k); a lane
+// holds AP_ROWS x JT outputs (frames lane, lane + 32, ...).
+constexpr int AP_ROWS = 8;
+constexpr int AP_JT = 4;  // frames per lane: n <= 128
 __global__ void __launch_bounds__(BW_THREADS) k_bwd_apply(Geo g, const float* __restrict__ in,
                                                           const float* __restrict__ gout, const float* __restrict__ wts,
                                                           float* __restrict__ gin, PatchWork w, BwdWork b, int ysplit) {
@@ -277,8 +280,8 @@ __global__ void __launch_bounds__(BW_THREADS) k_bwd_apply(Geo g, const float* __
   const int n = g.cols, M = g.rows;
   float* K1 = smf;                        // n x n
   float* K2 = K1 + n * n;                 // n x n
-  float* xs = K2 + n * n;                 // [warps][AP_ROWS][n] centred rows
-  float* gs = xs + (BW_THREADS / 32) * AP_ROWS * n;  // [warps][AP_ROWS][n] Gb rows
+  float* xs = K1 + ((2 * n * n + 3) & ~3);  // [warps][n][AP_ROWS] centred rows, k-major (16-byte aligned)
+  float* gs = xs + (BW_THREADS / 32) * AP_ROWS * n;  // [warps][n][AP_ROWS] Gb rows, k-major
   float* mu = gs + (BW_THREADS / 32) * AP_ROWS * n;  // [n]
   float* uu = mu + n;                                // [n]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -308,25 +311,43 @@ __global__ void __launch_bounds__(BW_THREADS) k_bwd_apply(Geo g, const float* __
       const int r = r0 + q;
       base[q] = r < M ? row_voxel(g, o, r) * g.shape[3] + o[3] : -1;
       for (int t = lane; t < n; t += 32) {
-        xw[q * n + t] = base[q] >= 0 ? in[base[q] + t] - mu[t] : 0.f;
-        gw[q * n + t] = base[q] >= 0 ? gbar(gout, wts, base[q] + t, theta) : 0.f;
+        xw[t * AP_ROWS + q] = base[q] >= 0 ? in[base[q] + t] - mu[t] : 0.f;
+        gw[t * AP_ROWS + q] = base[q] >= 0 ? gbar(gout, wts, base[q] + t, theta) : 0.f;
       }
     }
     __syncwarp();
-    for (int j0 = 0; j0 < n; j0 += 32) {
-      const int j = j0 + lane;
-      float acc[AP_ROWS];
+    float acc[AP_ROWS][AP_JT];
 #pragma unroll
-      for (int q = 0; q < AP_ROWS; ++q) acc[q] = 0.f;
-      if (j < n) {
-        for (int k = 0; k < n; ++k) {
-          const float a1 = K1[k * n + j], a2 = K2[k * n + j];
+    for (int q = 0; q < AP_ROWS; ++q)
 #pragma unroll
-          for (int q = 0; q < AP_ROWS; ++q) acc[q] += xw[q * n + k] * a1 + gw[q * n + k] * a2;
-        }
+      for (int c = 0; c < AP_JT; ++c) acc[q][c] = 0.f;
+    for (int k = 0; k < n; ++k) {
+      float a1[AP_JT], a2[AP_JT];
 #pragma unroll
-        for (int q = 0; q < AP_ROWS; ++q)
-          if (base[q] >= 0) atomicAdd(gin + base[q] + j, acc[q] + uu[j]);
+      for (int c = 0; c < AP_JT; ++c) {
+        const int j = lane + 32 * c;
+        a1[c] = j < n ? K1[k * n + j] : 0.f;
+        a2[c] = j < n ? K2[k * n + j] : 0.f;
+      }
+      const float4* xk = reinterpret_cast<const float4*>(xw + k * AP_ROWS);
+      const float4* gk = reinterpret_cast<const float4*>(gw + k * AP_ROWS);
+#pragma unroll
+      for (int h = 0; h < AP_ROWS / 4; ++h) {
+        const float4 xv = xk[h], gv = gk[h];
+        const float xr[4] = {xv.x, xv.y, xv.z, xv.w}, gr[4] = {gv.x, gv.y, gv.z, gv.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+#pragma unroll
+          for (int c = 0; c < AP_JT; ++c) acc[4 * h + e][c] += xr[e] * a1[c] + gr[e] * a2[c];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < AP_ROWS; ++q) {
+      if (base[q] < 0) continue;
+#pragma unroll
+      for (int c = 0; c < AP_JT; ++c) {
+        const int j = lane + 32 * c;
+        if (j < n) atomicAdd(gin + base[q] + j, acc[q][c] + uu[j]);
       }
     }
     __syncwarp();
@@ -335,7 +356,8 @@ __global__ void __launch_bounds__(BW_THREADS) k_bwd_apply(Geo g, const float* __
 
 size_t bwd_small_smem(int n) { return sizeof(float) * ((size_t)3 * n * bw_ld(n) + 5 * (size_t)n); }
 size_t bwd_apply_smem(int n) {
-  return sizeof(float) * ((size_t)2 * n * n + 2 * (size_t)(BW_THREADS / 32) * AP_ROWS * n + 2 * (size_t)n);
+  return sizeof(float) * ((((size_t)2 * n * n + 3) & ~(size_t)3) + 2 * (size_t)(BW_THREADS / 32) * AP_ROWS * n +
+                          2 * (size_t)n);
 }
 bool bwd_supported(int n) { return n <= 128 && bwd_apply_smem(n) <= 227 * 1024 && bwd_small_smem(n) <= 227 * 1024; }
 
