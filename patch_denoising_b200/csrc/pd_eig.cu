@@ -20,6 +20,7 @@
 #include "pd_common.cuh"
 #include "pd_kernels.cuh"
 #include "pd_profile.cuh"
+#include "pd_rules.cuh"
 
 namespace pd {
 
@@ -938,49 +939,10 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
     __syncthreads();
     cta_eigs(d, e2, n, ti, idx, lam, ne);
     if (tid == 0) {
-      double l[10];
-      for (int i = 0; i < 10; ++i) l[i] = 0.0;
-      // ascending top eigenvalues of C / (M - 1); zero-padded if n < 10
-      for (int i = 0; i < ne; ++i) l[10 - ne + i] = (double)lam[i] * tscale / (M - 1.0);
-      int k = 0;
+      int k;
       double var;
-      if (ep.method == PD_METHOD_MPPCA) {
-        double s = 0.0;
-        for (int i = 0; i < 10; ++i) s += l[i];
-        double crit = (s / 10.0) * (4.0 * sqrt((10.0 - 0 + 1.0) / M));
-        while (k < 10 && crit < l[9 - k] - l[0]) {
-          ++k;
-          if (k < 10) {
-            double t = 0.0;
-            for (int i = 0; i < 10 - k; ++i) t += l[i];
-            crit = (t / (10 - k)) * (4.0 * sqrt((pt - k + 1.0) / M));
-          } else {
-            crit = nan("");
-          }
-        }
-        if (k < 10) {
-          double t = 0.0;
-          for (int i = 0; i < 10 - k; ++i) t += l[i];
-          var = t / (10 - k);
-        } else {
-          var = nan("");
-        }
-        const double cut = var * ep.threshold_scale * ep.threshold_scale;
-        int r = 0;
-        for (int i = 0; i < 10; ++i) r += (l[i] > cut) ? 1 : 0;
-        k = r;
-      } else {
-        const double varest = w.prior[p];
-        double s = 0.0;
-        for (int i = 0; i < 10; ++i) s += l[i];
-        var = s / 10.0;
-        while (var > varest && k < 10 - 2) {
-          ++k;
-          double t = 0.0;
-          for (int i = 0; i < 10 - k; ++i) t += l[i];
-          var = t / (10 - k);
-        }
-      }
+      mp_hybrid_rule(ep.method == PD_METHOD_MPPCA, ep.threshold_scale, ep.method == PD_METHOD_HYBRID ? w.prior[p] : 0.0,
+                     lam, ne, tscale, M, pt, &k, &var);
       w.rank[p] = k;
       w.noise[p] = (float)var;
       const int act = k < ne ? k : ne;
