@@ -398,9 +398,17 @@ def ours_arm(args, rank, world):
         # launch lists and captures (no timing line: numbers under a profiler are
         # not bench values)
         for i in range(args.profile_calls):
-            out = step(args.precision, xd, i)[0][0]
+            if args.profile_method == "adaptive":  # the bench's adaptive SURE call (10 candidate gammas)
+                from patch_denoising_b200.space_time import AdaptiveDenoiser
+
+                np.random.seed(i)
+                out = AdaptiveDenoiser(PATCH, OVERLAP, method="SURE", precision=args.precision).denoise(
+                    xd, noise_std=NOISE, gamma0=np.linspace(1, 5, 10))[0]
+            else:
+                out = step(args.precision, xd, i)[0][0]
         torch.cuda.synchronize()
-        print(f"profile calls: {args.profile_calls} x {args.precision}, mean |out| {float(torch.nanmean(out.abs())):.6g}")
+        print(f"profile calls: {args.profile_calls} x {args.profile_method} {args.precision}, "
+              f"mean |out| {float(torch.nanmean(out.abs())):.6g}")
         return
 
     def timed(precision, prof=False):
@@ -573,6 +581,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the other configurations' timings")
     ap.add_argument("--profile-calls", type=int, default=0, metavar="K",
                     help="run K device-resident calls of the benchmarked workload and exit (for ncu)")
+    ap.add_argument("--profile-method", choices=["nordic", "adaptive"], default="nordic",
+                    help="the call --profile-calls repeats: the NORDIC step or the adaptive SURE call")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -50,19 +50,27 @@ __device__ __forceinline__ void st_pack2(__nv_bfloat16* hi, __nv_bfloat16* lo, i
   *reinterpret_cast<__nv_bfloat162*>(lo + off) = __floats2bfloat162_rn(a - f.x, b - f.y);
 }
 
-// grid: patches x tiles^2 (64 x 64 entries of K), 256 threads; a thread holds
-// 4 consecutive i x 4 j (strided by 16).
+// grid: patches x the tiles (ti >= tj) of K's lower triangle (64 x 64
+// entries each), 256 threads; a thread holds 4 consecutive i x 4 j (strided by
+// 16). K is Hermitian: an off-diagonal tile also writes its mirror (j, i).
 template <bool CPLX>
 __global__ void __launch_bounds__(256) k_synth_coef(int n, PatchWork w, int64_t kn, __nv_bfloat16* __restrict__ ahi,
                                                     __nv_bfloat16* __restrict__ alo) {
   using T = typename Elem<CPLX>::T;
-  __shared__ T vi[CF_A][CF_T];
-  __shared__ T vj[CF_A][CF_T];
+  __shared__ __align__(16) T vi[CF_A][CF_T];
+  __shared__ __align__(16) T vj[CF_A][CF_T];
   __shared__ float cs[CF_A];
   const int tiles = (n + CF_T - 1) / CF_T;
-  const int p = (int)(blockIdx.x / (unsigned)(tiles * tiles));
-  const int t = (int)(blockIdx.x - (unsigned)p * (unsigned)(tiles * tiles));
-  const int i0 = (t % tiles) * CF_T, j0 = (t / tiles) * CF_T;
+  const int per = tiles * (tiles + 1) / 2;
+  const int p = (int)(blockIdx.x / (unsigned)per);
+  int t = (int)(blockIdx.x - (unsigned)p * (unsigned)per);
+  int ti = 0;
+  while (t > ti) {  // lower-triangle tile t -> (ti, tj), tj <= ti
+    t -= ti + 1;
+    ++ti;
+  }
+  const int tj = t;
+  const int i0 = ti * CF_T, j0 = tj * CF_T;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int act = w.n_active[p];
   const float* vb = w.vec + (int64_t)p * w.vec_stride;
@@ -97,9 +105,24 @@ __global__ void __launch_bounds__(256) k_synth_coef(int n, PatchWork w, int64_t 
     for (int aa = 0; aa < CF_A; ++aa) {
       const float c = cs[aa];
       T x[4], y[4];
+      // the thread's four consecutive i in 16-byte loads (a half-warp shares them)
+      if constexpr (CPLX) {
+        const float4 u0 = *reinterpret_cast<const float4*>(&vi[aa][4 * tx]);
+        const float4 u1 = *reinterpret_cast<const float4*>(&vi[aa][4 * tx + 2]);
+        x[0] = cf{u0.x, u0.y};
+        x[1] = cf{u0.z, u0.w};
+        x[2] = cf{u1.x, u1.y};
+        x[3] = cf{u1.z, u1.w};
+      } else {
+        const float4 u0 = *reinterpret_cast<const float4*>(&vi[aa][4 * tx]);
+        x[0] = u0.x;
+        x[1] = u0.y;
+        x[2] = u0.z;
+        x[3] = u0.w;
+      }
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        x[q] = vi[aa][4 * tx + q] * c;
+        x[q] = x[q] * c;
         y[q] = vj[aa][ty + 16 * q];
       }
 #pragma unroll
@@ -112,10 +135,12 @@ __global__ void __launch_bounds__(256) k_synth_coef(int n, PatchWork w, int64_t 
     }
   }
   // A[j][i] = K_emb[i][j]: complex entry (i, j) = a + ib fills rows 2j, 2j+1,
-  // columns 2i, 2i+1 with [a, -b] and [b, a]
+  // columns 2i, 2i+1 with [a, -b] and [b, a]; its mirror (j, i) = a - ib fills
+  // rows 2i, 2i+1, columns 2j, 2j+1 with [a, b] and [-b, a]
   __nv_bfloat16* hp = ahi + (int64_t)p * (CPLX ? 2 * n : n) * kn;
   __nv_bfloat16* lp = alo + (int64_t)p * (CPLX ? 2 * n : n) * kn;
   const int ib = i0 + 4 * tx;
+  const bool mirror = ti != tj;
 #pragma unroll
   for (int qj = 0; qj < 4; ++qj) {
     const int j = j0 + ty + 16 * qj;
@@ -129,6 +154,11 @@ __global__ void __launch_bounds__(256) k_synth_coef(int n, PatchWork w, int64_t 
         const cf k = ib + qi < n ? acc[qi][qj] : cf{0.f, 0.f};
         st_pack2(hp, lp, r0 + c, k.x, -k.y);
         st_pack2(hp, lp, r1 + c, k.y, k.x);
+        if (mirror && ib + qi < n) {
+          const int64_t m0 = (int64_t)(2 * (ib + qi)) * kn + 2 * j;
+          st_pack2(hp, lp, m0, k.x, k.y);
+          st_pack2(hp, lp, m0 + kn, -k.y, k.x);
+        }
       }
     } else {
       const int64_t r0 = (int64_t)j * kn;
@@ -137,6 +167,16 @@ __global__ void __launch_bounds__(256) k_synth_coef(int n, PatchWork w, int64_t 
         const int64_t c = ib + qi;
         if (c >= kn) break;
         st_pack2(hp, lp, r0 + c, ib + qi < n ? acc[qi][qj] : 0.f, ib + qi + 1 < n ? acc[qi + 1][qj] : 0.f);
+      }
+      if (mirror) {
+#pragma unroll
+        for (int qi = 0; qi < 4; ++qi) {
+          if (ib + qi >= n) break;
+          const int64_t m0 = (int64_t)(ib + qi) * kn + j;
+          const __nv_bfloat16 h = __float2bfloat16_rn(acc[qi][qj]);
+          hp[m0] = h;
+          lp[m0] = __float2bfloat16_rn(acc[qi][qj] - __bfloat162float(h));
+        }
       }
     }
   }
@@ -369,7 +409,7 @@ cudaError_t launch_synth_tc(const Geo& g, bool cplx, const PatchWork& w, const S
   __nv_bfloat16* base = reinterpret_cast<__nv_bfloat16*>(w.packed);
   const int n = g.cols;
   const int tiles = (n + CF_T - 1) / CF_T;
-  const unsigned cgrid = (unsigned)((int64_t)w.count * tiles * tiles);
+  const unsigned cgrid = (unsigned)((int64_t)w.count * tiles * (tiles + 1) / 2);
   if (cplx)
     PD_TIMED("synth_coef", s,
              k_synth_coef<true><<<cgrid, 256, 0, s>>>(n, w, L.kn, base + L.coef_hi, base + L.coef_lo));
