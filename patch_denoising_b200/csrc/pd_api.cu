@@ -754,7 +754,12 @@ pd_status pd_denoise_batch(const pd_volume* vols, int32_t n_vols, const pd_param
   // chunks of at most `chunk` patches that do not mix the kernels' frame-count
   // classes (their register slots per lane are sized by the largest frame count
   // of a launch), in work-list order
-  auto frame_class = [](int64_t n) { return n <= 64 ? 0 : n <= 128 ? 1 : n <= 224 ? 2 : n <= 320 ? 3 : 4; };
+  // (the classes also separate the patches the eigensolver runs in small CTAs,
+  // so a batched patch takes the same kernel variant as a one-volume call)
+  auto frame_class = [cplx](int64_t n) {
+    const int c = n <= 64 ? 0 : n <= 128 ? 1 : n <= 224 ? 2 : n <= 320 ? 3 : 4;
+    return 2 * c + (eig_small(cplx, (int)n) ? 0 : 1);
+  };
   std::vector<std::pair<int64_t, int64_t>> pieces;  // (offset, count)
   {
     int64_t start = 0, len = 0;
@@ -797,8 +802,7 @@ pd_status pd_denoise_batch(const pd_volume* vols, int32_t n_vols, const pd_param
       if (c == 0 || f + c <= off || f >= off + cnt) continue;
       nc = std::max(nc, (int)t.v[k].d.g.cols);
       mc = std::max(mc, (int)t.v[k].d.g.rows);
-      bool in_smem;
-      esm = std::max(esm, eig_smem_bytes(cplx, (int)t.v[k].d.g.cols, &in_smem));
+      esm = std::max(esm, eig_launch_smem(cplx, (int)t.v[k].d.g.cols));
     }
     G.rows = mc;
     G.cols = nc;

@@ -34,7 +34,10 @@ struct EigLayout {
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
 
-__host__ __device__ inline EigLayout eig_layout(bool cplx, int n, bool in_smem) {
+// th: the CTA's threads. pw holds a row of partial products per warp in the
+// tridiagonalisation, and later the adaptive rule's 3 n doubles and the block
+// re-orthogonalisation's 16 n floats: at least 64 n bytes.
+__host__ __device__ inline EigLayout eig_layout(bool cplx, int n, bool in_smem, int th = EIG_THREADS) {
   const size_t es = cplx ? 8 : 4;
   EigLayout L;
   size_t o = 0;
@@ -53,7 +56,10 @@ __host__ __device__ inline EigLayout eig_layout(bool cplx, int n, bool in_smem) 
   L.wb = o;
   o += al16(es * 2 * n);
   L.pw = o;
-  o += al16(es * n * (EIG_THREADS / 32));
+  {
+    const size_t per_warp = es * n * (size_t)(th / 32), scratch = 64 * (size_t)n;
+    o += al16(per_warp > scratch ? per_warp : scratch);
+  }
   L.pd = o;
   o += al16(es * n);
   L.idx = o;
@@ -107,7 +113,7 @@ __device__ __forceinline__ float bmax_f(float v) {
   __syncthreads();
   if (lane == 0) red[w] = v;
   __syncthreads();
-  float r = lane < EIG_NW ? red[lane] : -FLT_MAX;
+  float r = lane < (int)((blockDim.x + 31) >> 5) ? red[lane] : -FLT_MAX;
   return warp_max(r);
 }
 __device__ __forceinline__ float warp_min(float v) {
@@ -149,24 +155,24 @@ template <>
 __device__ __forceinline__ cf shfl_idx<cf>(cf v, int src) {
   return cf{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
 }
-template <bool CPLX, int NS>
+template <bool CPLX, int NS, int TH>
 __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float* e, typename Elem<CPLX>::T* tau,
                                typename Elem<CPLX>::T* vb, typename Elem<CPLX>::T* wb,
                                typename Elem<CPLX>::T* pw, typename Elem<CPLX>::T* pd) {
   using T = typename Elem<CPLX>::T;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  __shared__ T s_red[EIG_NW];     // per-warp partials of (tau p)^H v
-  __shared__ float s_x2[EIG_NW];  // per-warp partials of the column norm
+  __shared__ T s_red[(TH / 32)];     // per-warp partials of (tau p)^H v
+  __shared__ float s_x2[(TH / 32)];  // per-warp partials of the column norm
   __shared__ T s_sub;             // A(j+1, j) after its last update
   T one;
   if constexpr (CPLX) one = cf{1.f, 0.f};
   else one = 1.f;
   // buffer 1 holds "step -1": v = w = 0, so the first pending update is exactly zero
-  for (int i = tid; i < 2 * n; i += EIG_THREADS) {
+  for (int i = tid; i < 2 * n; i += TH) {
     vb[i] = zero<T>();
     wb[i] = zero<T>();
   }
-  if (tid < EIG_NW) s_red[tid] = zero<T>();
+  if (tid < (TH / 32)) s_red[tid] = zero<T>();
   T tau_prev = zero<T>();  // tau of the previous step (every thread)
   __syncthreads();
   for (int j = 0; j < n - 1; ++j) {
@@ -179,10 +185,10 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
     // ---- phase 1 (all): finish column j (thread t owns row j + t), build reflector j
     T al, tj = zero<T>();
     {
-      T dot = lane < EIG_NW ? s_red[lane] : zero<T>();
+      T dot = lane < (TH / 32) ? s_red[lane] : zero<T>();
       dot = warp_sum(dot);
       al = mul(tau_prev, dot) * -0.5f;  // w_{j-1} = tau p + al v
-      const int r = j + tid;            // n - j <= n <= EIG_THREADS rows
+      const int r = j + tid;            // n - j <= n <= TH rows
       T a = zero<T>();
       float x2 = 0.f;
       if (r < n) {
@@ -198,7 +204,7 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
       if (tid == 1) s_sub = a;  // A(j+1, j)
       if (tid == 0) d[j] = re(a);
       __syncthreads();
-      float xn2 = lane < EIG_NW ? s_x2[lane] : 0.f;
+      float xn2 = lane < (TH / 32) ? s_x2[lane] : 0.f;
       xn2 = warp_sum(xn2);
       const T alpha = s_sub;
       const float ar = re(alpha);
@@ -252,12 +258,12 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
           vn[s] = vc[r];
         }
       }
-      for (int k0 = warp; k0 < m; k0 += 8 * EIG_NW) {
+      for (int k0 = warp; k0 < m; k0 += 8 * (TH / 32)) {
         T dp[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           dp[q] = zero<T>();
-          const int k = k0 + q * EIG_NW;
+          const int k = k0 + q * (TH / 32);
           if (k < m) {
             const int c = j + 1 + k;
             const T vok = vp[c];
@@ -280,7 +286,7 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
         }
         int slot;
         const T tot = reduce_scatter8<T>(dp, lane, &slot);
-        const int k = k0 + slot * EIG_NW;
+        const int k = k0 + slot * (TH / 32);
         if ((lane & 3) == 0 && k < m) pd[j + 1 + k] = tot;
       }
       T* mine = pw + warp * n;
@@ -298,7 +304,7 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
         const int r = j + 1 + tid;
         T pv = pd[r];
 #pragma unroll 4
-        for (int w = 0; w < EIG_NW; ++w) pv = pv + pw[w * n + r];
+        for (int w = 0; w < (TH / 32); ++w) pv = pv + pw[w * n + r];
         const T wv = mul(tj, pv);
         wc[r] = wv;
         dpart = cmulc(wv, vc[r]);
@@ -315,7 +321,7 @@ __device__ void tridiagonalize(typename Elem<CPLX>::T* A, int n, float* d, float
     } else {
       // the last diagonal entry takes the update of step n-2
       T dot = zero<T>();
-      for (int w = 0; w < EIG_NW; ++w) dot = dot + s_red[w];
+      for (int w = 0; w < (TH / 32); ++w) dot = dot + s_red[w];
       const T al = mul(tau[n - 2], dot) * -0.5f;
       const int c = (n - 2) & 1;
       const T v = vb[c * n + n - 1];
@@ -366,10 +372,11 @@ struct TriInfo {
 };
 
 // Eigenvalues at indices idx[0..cnt) into out[]; warps take entries.
+template <int TH>
 __device__ void cta_eigs(const float* d, const float* e2, int n, const TriInfo& ti, const int* idx,
                          float* out, int cnt) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int q = warp; q < cnt; q += EIG_NW) {
+  for (int q = warp; q < cnt; q += (TH / 32)) {
     const float v = warp_kth(d, e2, n, idx[q], ti.gl, ti.gu, ti.pivmin, ti.abstol);
     if (lane == 0) out[q] = v;
   }
@@ -392,7 +399,7 @@ constexpr int LANCZOS_STEPS = 48;
 // Q: (min(n, LANCZOS_STEPS) + 1) * n floats of scratch; al, be, be2: n floats each.
 // FULL = false: A is packed lower (ld unused); true: a full row-major square
 // with leading dimension ld (odd, so a thread per row reads conflict-free).
-template <bool FULL>
+template <bool FULL, int TH>
 __device__ float lanczos_top1(const float* A, int n, int ld, float* Q, float* al, float* be, float* be2) {
   __shared__ float s_coef[LANCZOS_STEPS];
   __shared__ float s_val;
@@ -400,7 +407,7 @@ __device__ float lanczos_top1(const float* A, int n, int ld, float* Q, float* al
   const int kmax = n < LANCZOS_STEPS ? n : LANCZOS_STEPS;
   float* wv = Q + (int64_t)kmax * n;
   float part = 0.f;
-  for (int i = tid; i < n; i += EIG_THREADS) {
+  for (int i = tid; i < n; i += TH) {
     uint32_t h = (uint32_t)(i + 7) * 2654435761u;
     h ^= h >> 13;
     h *= 0x5bd1e995u;
@@ -410,14 +417,14 @@ __device__ float lanczos_top1(const float* A, int n, int ld, float* Q, float* al
     part += x * x;
   }
   const float nr = rsqrtf(bsum_f(part));
-  for (int i = tid; i < n; i += EIG_THREADS) Q[i] *= nr;
+  for (int i = tid; i < n; i += TH) Q[i] *= nr;
   __syncthreads();
   int kk = kmax;
   for (int j = 0; j < kmax; ++j) {
     const float* qj = Q + (int64_t)j * n;
     if constexpr (FULL) {
       // w = A q_j: a thread per row
-      for (int r = tid; r < n; r += EIG_THREADS) {
+      for (int r = tid; r < n; r += TH) {
         const float* row = A + (int64_t)r * ld;
         float s0 = 0.f, s1 = 0.f;
         int k = 0;
@@ -430,7 +437,7 @@ __device__ float lanczos_top1(const float* A, int n, int ld, float* Q, float* al
       }
     } else {
       // w = A q_j: a warp per row, lanes over the columns
-      for (int r = warp; r < n; r += EIG_NW) {
+      for (int r = warp; r < n; r += (TH / 32)) {
         float s = 0.f;
         for (int k = lane; k < n; k += 32) s += A[k <= r ? pk(r, k, n) : pk(k, r, n)] * qj[k];
         s = warp_sum(s);
@@ -440,7 +447,7 @@ __device__ float lanczos_top1(const float* A, int n, int ld, float* Q, float* al
     __syncthreads();
     float b2p = 0.f;
     for (int pass = 0; pass < 2; ++pass) {
-      for (int c = warp; c <= j; c += EIG_NW) {
+      for (int c = warp; c <= j; c += (TH / 32)) {
         const float* qc = Q + (int64_t)c * n;
         float s = 0.f;
         for (int i = lane; i < n; i += 32) s += qc[i] * wv[i];
@@ -450,7 +457,7 @@ __device__ float lanczos_top1(const float* A, int n, int ld, float* Q, float* al
       __syncthreads();
       if (pass == 0 && tid == 0) al[j] = s_coef[j];
       b2p = 0.f;
-      for (int i = tid; i < n; i += EIG_THREADS) {
+      for (int i = tid; i < n; i += TH) {
         float s = wv[i];
 #pragma unroll 8
         for (int c = 0; c <= j; ++c) s -= s_coef[c] * Q[(int64_t)c * n + i];
@@ -470,7 +477,7 @@ __device__ float lanczos_top1(const float* A, int n, int ld, float* Q, float* al
     }
     const float inv = rsqrtf(b2);
     float* qn = Q + (int64_t)(j + 1) * n;
-    for (int i = tid; i < n; i += EIG_THREADS) qn[i] = wv[i] * inv;
+    for (int i = tid; i < n; i += TH) qn[i] = wv[i] * inv;
     __syncthreads();
   }
   __syncthreads();
@@ -673,6 +680,7 @@ __device__ double ad_minimize(const F& f, double x0, double xlo, double xhi) {
 // the (G)SURE minimisation and the shrinkage coefficients. Compiled only into
 // k_eig's ADAPT instantiation, so that its FP64 search leaves the other
 // methods' kernels as they are. scratch: 3 n doubles of shared memory.
+template <int TH>
 __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adaptive& ad, const PatchWork& w, int p,
                                               int n, const float* d,
                                            const float* e2, const TriInfo& ti, int* idx, float* lam, int* aidx,
@@ -689,9 +697,9 @@ __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adap
     if (tid == 0) s_c0q = sturm_count(d, e2, n, (float)(tau * tau / tscale * (1.0 - CAND_MARGIN)), ti.pivmin);
     __syncthreads();
     const int nc = n - s_c0q;
-    for (int i = tid; i < nc; i += EIG_THREADS) idx[i] = s_c0q + i;
+    for (int i = tid; i < nc; i += TH) idx[i] = s_c0q + i;
     __syncthreads();
-    cta_eigs(d, e2, n, ti, idx, lam, nc);
+    cta_eigs<TH>(d, e2, n, ti, idx, lam, nc);
     if (tid == 0) {
       const double gq = ad.gamma[0], lt = log(tau);
       int r = 0;
@@ -714,9 +722,9 @@ __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adap
   }
   // the whole spectrum: singular values s = sqrt(eigenvalue) in numpy.svd's
   // (descending) order, min(M, n) of them
-  for (int i = tid; i < n; i += EIG_THREADS) idx[i] = i;
+  for (int i = tid; i < n; i += TH) idx[i] = i;
   __syncthreads();
-  cta_eigs(d, e2, n, ti, idx, lam, n);
+  cta_eigs<TH>(d, e2, n, ti, idx, lam, n);
   const int nv = ep.rows < n ? ep.rows : n;
   double* sv = scratch;
   double* lsv = sv + n;
@@ -724,12 +732,12 @@ __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adap
   // a centred M x T patch with M <= T has rank M - 1 at most: its singular
   // values from index M - 1 on are zero (the Gram's rounding leaves them small)
   const int nz = ep.rows <= n ? ep.rows - 1 : nv;
-  for (int k = tid; k < nv; k += EIG_THREADS) {
+  for (int k = tid; k < nv; k += TH) {
     sv[k] = k < nz ? sqrt(fmax((double)lam[n - 1 - k] * tscale, 0.0)) : 0.0;
     lsv[k] = log(sv[k]);
   }
   __syncthreads();
-  for (int k = tid; k < nv; k += EIG_THREADS) {
+  for (int k = tid; k < nv; k += TH) {
     const double a2 = sv[k] * sv[k];
     double acc = 0.0;
     if (a2 > 0.0)  // zero singular values are skipped by the cost (their si is unused)
@@ -773,7 +781,7 @@ __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adap
       const double med = (nv & 1) ? sv[nv / 2] : 0.5 * (sv[nv / 2 - 1] + sv[nv / 2]);
       x0 = med > 0.0 ? log(med) : xlo;  // a median of zeros: start at the smallest positive value
     }
-    for (int q = warp; q < ad.n_gamma; q += EIG_NW) {
+    for (int q = warp; q < ad.n_gamma; q += (TH / 32)) {
       const double gq = ad.gamma[q];
       const double x = ad_minimize([&](double xx) { return ad_cost(c, xx, gq); }, x0, xlo, xhi);
       const double cost = ad_cost(c, x, gq);
@@ -818,11 +826,11 @@ __device__ __forceinline__ void adaptive_rule(const EigParams& ep, const pd_adap
 // ---------------------------------------------------------------------------
 // The kernel
 // ---------------------------------------------------------------------------
-template <bool CPLX, int NS, bool ADAPT>
+template <bool CPLX, int NS, bool ADAPT, int TH>
 // ADAPT: with the adaptive rule (PD_METHOD_ADAPTIVE launches only).
 // in_smem: bit 0 = the packed matrix lives in shared memory, bit 1 = the
 // Lanczos basis of the top-1 mode does too (after the layout's end).
-__global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, PatchWork w, int in_smem,
+__global__ void __launch_bounds__(TH, TH >= 512 ? 1 : 4) k_eig(int n, EigParams ep, PatchWork w, int in_smem,
                                                        pd_adaptive ad) {
   using T = typename Elem<CPLX>::T;
   extern __shared__ __align__(16) unsigned char sm[];
@@ -839,9 +847,9 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
     ep.mp_median = v.mp_median;
     uint32_t dyn;
     asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-    in_smem = eig_layout(CPLX, n, true).total <= dyn ? 1 : 0;
+    in_smem = eig_layout(CPLX, n, true, TH).total <= dyn ? 1 : 0;
   }
-  const EigLayout L = eig_layout(CPLX, n, (in_smem & 1) != 0);
+  const EigLayout L = eig_layout(CPLX, n, (in_smem & 1) != 0, TH);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (ep.only_unfinished && w.n_active[p] >= 0) return;  // solved by k_sub
   T* G = reinterpret_cast<T*>(w.gram + (int64_t)p * w.gram_stride);
@@ -866,23 +874,23 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
 
   const int64_t np = pk_size(n);
   if (in_smem & 1) {
-    for (int64_t i = tid; i < np; i += EIG_THREADS) A[i] = G[i];
+    for (int64_t i = tid; i < np; i += TH) A[i] = G[i];
     __syncthreads();
   }
   // scale by 1 / max diagonal
   float md = 0.f;
-  for (int i = tid; i < n; i += EIG_THREADS) md = fmaxf(md, re(A[pk(i, i, n)]));
+  for (int i = tid; i < n; i += TH) md = fmaxf(md, re(A[pk(i, i, n)]));
   md = bmax_f(md);
   const float sc = md > 0.f ? 1.f / md : 1.f;
   if (tid == 0) s_scale_true = md > 0.f ? (double)md : 1.0;
   __syncthreads();
-  for (int64_t i = tid; i < np; i += EIG_THREADS) A[i] = A[i] * sc;
+  for (int64_t i = tid; i < np; i += TH) A[i] = A[i] * sc;
   __syncthreads();
 
   if constexpr (!CPLX) {
     if (ep.method == EIG_MODE_TOP1) {  // Monte-Carlo level: top eigenvalue only
       float* Q = (in_smem & 2) ? reinterpret_cast<float*>(sm + L.total) : w.vec + (int64_t)p * w.vec_stride;
-      const float lam1 = lanczos_top1<false>(A, n, 0, Q, d, e, e2);
+      const float lam1 = lanczos_top1<false, TH>(A, n, 0, Q, d, e, e2);
       if (tid == 0) {
         w.prior[p] = (double)lam1 * s_scale_true;
         w.n_active[p] = 0;
@@ -890,11 +898,11 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
       return;
     }
   }
-  tridiagonalize<CPLX, NS>(A, n, d, e, tau, vb, wb, pw, pd);
+  tridiagonalize<CPLX, NS, TH>(A, n, d, e, tau, vb, wb, pw, pd);
 
   // e2, Gershgorin bounds, tolerances
   float glo = FLT_MAX, ghi = -FLT_MAX, emax = 0.f, tn = 0.f;
-  for (int i = tid; i < n; i += EIG_THREADS) {
+  for (int i = tid; i < n; i += TH) {
     const float el = i > 0 ? fabsf(e[i - 1]) : 0.f;
     const float er = i < n - 1 ? fabsf(e[i]) : 0.f;
     if (i < n - 1) e2[i] = e[i] * e[i];
@@ -920,10 +928,10 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
 
   // ---------------------------------------------------------------- decisions
   if (ADAPT && ep.method == EIG_MODE_FULL) {  // the whole decomposition (ADAPT instantiation)
-    for (int i = tid; i < n; i += EIG_THREADS) idx[i] = i;
+    for (int i = tid; i < n; i += TH) idx[i] = i;
     __syncthreads();
-    cta_eigs(d, e2, n, ti, idx, lam, n);
-    for (int a = tid; a < n; a += EIG_THREADS) {
+    cta_eigs<TH>(d, e2, n, ti, idx, lam, n);
+    for (int a = tid; a < n; a += TH) {
       aidx[a] = n - 1 - a;
       alam[a] = lam[n - 1 - a];
       acoef[a] = (float)((double)lam[n - 1 - a] * tscale);
@@ -931,13 +939,13 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
     if (tid == 0) s_act = n;
     __syncthreads();
   } else if (ADAPT && ep.method == PD_METHOD_ADAPTIVE) {  // compiled into the ADAPT instantiation only
-    adaptive_rule(ep, ad, w, p, n, d, e2, ti, idx, lam, aidx, alam, acoef, reinterpret_cast<double*>(pw), tscale, M,
+    adaptive_rule<TH>(ep, ad, w, p, n, d, e2, ti, idx, lam, aidx, alam, acoef, reinterpret_cast<double*>(pw), tscale, M,
                   pt, &s_act);
   } else if (ep.method == PD_METHOD_MPPCA || ep.method == PD_METHOD_HYBRID) {
     const int ne = n < 10 ? n : 10;
     if (tid < ne) idx[tid] = n - ne + tid;
     __syncthreads();
-    cta_eigs(d, e2, n, ti, idx, lam, ne);
+    cta_eigs<TH>(d, e2, n, ti, idx, lam, ne);
     if (tid == 0) {
       int k;
       double var;
@@ -962,9 +970,9 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
     }
     __syncthreads();
     const int nc = n - s_c0;
-    for (int i = tid; i < nc; i += EIG_THREADS) idx[i] = s_c0 + i;
+    for (int i = tid; i < nc; i += TH) idx[i] = s_c0 + i;
     __syncthreads();
-    cta_eigs(d, e2, n, ti, idx, lam, nc);
+    cta_eigs<TH>(d, e2, n, ti, idx, lam, nc);
     if (tid == 0) {
       int r = 0;
       for (int i = nc - 1; i >= 0; --i) {
@@ -993,7 +1001,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
       }
     }
     __syncthreads();
-    cta_eigs(d, e2, n, ti, idx, lam, s_cnt);
+    cta_eigs<TH>(d, e2, n, ti, idx, lam, s_cnt);
     if (tid == 0) {
       double smed;
       if (n & 1)
@@ -1015,10 +1023,10 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
     }
     __syncthreads();
     const int ntop = s_c0, nbot = s_c1;
-    for (int i = tid; i < nbot; i += EIG_THREADS) idx[i] = i;
-    for (int i = tid; i < ntop; i += EIG_THREADS) idx[nbot + i] = n - ntop + i;
+    for (int i = tid; i < nbot; i += TH) idx[i] = i;
+    for (int i = tid; i < ntop; i += TH) idx[nbot + i] = n - ntop + i;
     __syncthreads();
-    cta_eigs(d, e2, n, ti, idx, lam, nbot + ntop);
+    cta_eigs<TH>(d, e2, n, ti, idx, lam, nbot + ntop);
     if (tid == 0) {
       const double scale = s_x0;
       const double beta = pt / M;
@@ -1047,7 +1055,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
   const int act = s_act;
   const int n2 = 2 * n;
   float* vbase = w.vec + (int64_t)p * w.vec_stride;
-  for (int a = tid; a < act; a += EIG_THREADS) {
+  for (int a = tid; a < act; a += TH) {
     float* z = vbase + (int64_t)a * n2;  // z[0..n): vector (first D-)
     float* Dp = z + n;                   // D+ scratch
     const float lm = alam[a];
@@ -1095,14 +1103,14 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
     // replaced by inverse iteration from a pseudo-random start; normalised
     auto finish = [&](float* za, int a, int cstart) {
       float part = 0.f;
-      for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * za[i];
+      for (int i = tid; i < n; i += TH) part += za[i] * za[i];
       float nr = sqrtf(bsum_f(part));
       if (nr < 0.05f) {
         // collapsed: inverse iteration from a pseudo-random start, orthogonalised
         const float* Dp = za + n;
         for (int it = 0; it < 3; ++it) {
           if (it == 0)
-            for (int i = tid; i < n; i += EIG_THREADS) {
+            for (int i = tid; i < n; i += TH) {
               uint32_t h = (uint32_t)(i + 1) * 2654435761u ^ (uint32_t)(a + 7) * 40503u;
               h ^= h >> 13;
               h *= 0x5bd1e995u;
@@ -1113,9 +1121,9 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
           for (int b = cstart; b < a; ++b) {
             const float* zb = vbase + (int64_t)b * n2;
             float pp = 0.f;
-            for (int i = tid; i < n; i += EIG_THREADS) pp += za[i] * zb[i];
+            for (int i = tid; i < n; i += TH) pp += za[i] * zb[i];
             const float dt = bsum_f(pp);
-            for (int i = tid; i < n; i += EIG_THREADS) za[i] -= dt * zb[i];
+            for (int i = tid; i < n; i += TH) za[i] -= dt * zb[i];
             __syncthreads();
           }
           if (tid == 0) {  // solve (T - lam I) x = za with T - lam I = L D L^T
@@ -1125,25 +1133,25 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
           }
           __syncthreads();
           float pp = 0.f;
-          for (int i = tid; i < n; i += EIG_THREADS) pp += za[i] * za[i];
+          for (int i = tid; i < n; i += TH) pp += za[i] * za[i];
           const float iv = rsqrtf(bsum_f(pp));
-          for (int i = tid; i < n; i += EIG_THREADS) za[i] *= iv;
+          for (int i = tid; i < n; i += TH) za[i] *= iv;
           __syncthreads();
         }
         for (int b = cstart; b < a; ++b) {
           const float* zb = vbase + (int64_t)b * n2;
           float pp = 0.f;
-          for (int i = tid; i < n; i += EIG_THREADS) pp += za[i] * zb[i];
+          for (int i = tid; i < n; i += TH) pp += za[i] * zb[i];
           const float dt = bsum_f(pp);
-          for (int i = tid; i < n; i += EIG_THREADS) za[i] -= dt * zb[i];
+          for (int i = tid; i < n; i += TH) za[i] -= dt * zb[i];
           __syncthreads();
         }
         part = 0.f;
-        for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * za[i];
+        for (int i = tid; i < n; i += TH) part += za[i] * za[i];
         nr = sqrtf(bsum_f(part));
       }
       const float iv = nr > 0.f ? 1.f / nr : 0.f;
-      for (int i = tid; i < n; i += EIG_THREADS) za[i] *= iv;
+      for (int i = tid; i < n; i += TH) za[i] *= iv;
       __syncthreads();
     };
     if constexpr (ADAPT) {
@@ -1168,13 +1176,13 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
       for (int a0 = 1; a0 < act; a0 += RB) {
         const int nb = min(RB, act - a0);
         const int lo = cst[a0];
-        for (int q = tid; q < nb * n; q += EIG_THREADS) {
+        for (int q = tid; q < nb * n; q += TH) {
           const int k = q / n, i = q - k * n;
           blk[k * n + i] = vbase[(int64_t)(a0 + k) * n2 + i];
         }
         __syncthreads();
         for (int pass = 0; pass < 2 && lo < a0; ++pass) {
-          for (int b = lo + warp; b < a0; b += EIG_NW) {
+          for (int b = lo + warp; b < a0; b += (TH / 32)) {
             const float* zb = vbase + (int64_t)b * n2;
             float dp[RB];
 #pragma unroll
@@ -1193,7 +1201,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
             }
           }
           __syncthreads();
-          for (int i = tid; i < n; i += EIG_THREADS) {
+          for (int i = tid; i < n; i += TH) {
             float acc[RB];
 #pragma unroll
             for (int k = 0; k < RB; ++k) acc[k] = 0.f;
@@ -1219,24 +1227,24 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
           }
           const int j0 = max(cst[a], a0) - a0;
           for (int pass = 0; pass < 2 && j0 < k; ++pass) {
-            for (int j = j0 + warp; j < k; j += EIG_NW) {
+            for (int j = j0 + warp; j < k; j += (TH / 32)) {
               float dp = 0.f;
               for (int i = lane; i < n; i += 32) dp += blk[j * n + i] * blk[k * n + i];
               dp = warp_sum(dp);
               if (lane == 0) dots[j] = dp;
             }
             __syncthreads();
-            for (int i = tid; i < n; i += EIG_THREADS) {
+            for (int i = tid; i < n; i += TH) {
               float v = blk[k * n + i];
               for (int j = j0; j < k; ++j) v -= dots[j] * blk[j * n + i];
               blk[k * n + i] = v;
             }
             __syncthreads();
           }
-          for (int i = tid; i < n; i += EIG_THREADS) za[i] = blk[k * n + i];
+          for (int i = tid; i < n; i += TH) za[i] = blk[k * n + i];
           __syncthreads();
           finish(za, a, cst[a]);
-          for (int i = tid; i < n; i += EIG_THREADS) blk[k * n + i] = za[i];
+          for (int i = tid; i < n; i += TH) blk[k * n + i] = za[i];
           __syncthreads();
         }
       }
@@ -1251,9 +1259,9 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
         for (int b = cstart; b < a; ++b) {
           const float* zb = vbase + (int64_t)b * n2;
           float part = 0.f;
-          for (int i = tid; i < n; i += EIG_THREADS) part += za[i] * zb[i];
+          for (int i = tid; i < n; i += TH) part += za[i] * zb[i];
           const float dt = bsum_f(part);
-          for (int i = tid; i < n; i += EIG_THREADS) za[i] -= dt * zb[i];
+          for (int i = tid; i < n; i += TH) za[i] -= dt * zb[i];
           __syncthreads();
         }
         finish(za, a, cstart);
@@ -1266,7 +1274,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
   // and their VG dot products reduce in parallel (whole spectra: act = n).
   constexpr int VGR = 48 / (NS * (CPLX ? 2 : 1));
   constexpr int VG = VGR < 1 ? 1 : (VGR > 8 ? 8 : VGR);
-  for (int g0 = warp * VG; g0 < act; g0 += EIG_NW * VG) {
+  for (int g0 = warp * VG; g0 < act; g0 += (TH / 32) * VG) {
     T y[VG][NS];
 #pragma unroll
     for (int v = 0; v < VG; ++v) {
@@ -1323,7 +1331,7 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_eig(int n, EigParams ep, Pat
       }
     }
   }
-  for (int a = tid; a < act; a += EIG_THREADS) w.coef[(int64_t)p * w.n_stride + a] = acoef[a];
+  for (int a = tid; a < act; a += TH) w.coef[(int64_t)p * w.n_stride + a] = acoef[a];
   if (tid == 0) w.n_active[p] = act;
 }
 
@@ -1364,15 +1372,51 @@ __global__ void __launch_bounds__(EIG_THREADS, 1) k_top1(int n, PatchWork w) {
     }
   }
   __syncthreads();
-  const float lam = lanczos_top1<true>(F, n, ld, Q, al, be, be2);
+  const float lam = lanczos_top1<true, EIG_THREADS>(F, n, ld, Q, al, be, be2);
   if (tid == 0) {
     w.prior[p] = (double)lam * s_md;
     w.n_active[p] = 0;
   }
 }
 
+// Small patches (n <= 128, so a thread per row of the tridiagonalisation) run
+// 128-thread CTAs, four per SM when their layout fits EIG_SMALL_SMEM each: the
+// latency-bound steps of four patches overlap instead of one patch's steps
+// leaving the SM idle.
+constexpr int EIG_SMALL_THREADS = 128;
+constexpr size_t EIG_SMALL_SMEM = 227 * 1024 / 4 - 2048;
+
+bool eig_small(bool cplx, int n) {
+  return n <= EIG_SMALL_THREADS && eig_layout(cplx, n, true, EIG_SMALL_THREADS).total <= EIG_SMALL_SMEM;
+}
+
+size_t eig_launch_smem(bool cplx, int n) {
+  if (eig_small(cplx, n)) return eig_layout(cplx, n, true, EIG_SMALL_THREADS).total;
+  bool in_smem;
+  return eig_smem_bytes(cplx, n, &in_smem);
+}
+
+template <bool CPLX, int NS, int TH>
+static cudaError_t eig_launch(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s, const pd_adaptive* ad,
+                              size_t smem, int flags) {
+  auto kern = (ep.method == PD_METHOD_ADAPTIVE || ep.method == EIG_MODE_FULL) ? k_eig<CPLX, NS, true, TH>
+                                                                               : k_eig<CPLX, NS, false, TH>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  pd_adaptive a{};
+  if (ad) a = *ad;
+  PD_TIMED(ep.method == EIG_MODE_TOP1 ? "eig_mc" : "eig", s, kern<<<w.count, TH, smem, s>>>(n, ep, w, flags, a));
+  return cudaGetLastError();
+}
+
 template <bool CPLX, int NS>
 static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaStream_t s, const pd_adaptive* ad) {
+  if constexpr (NS * 32 <= EIG_SMALL_THREADS) {
+    const size_t small = eig_layout(CPLX, n, true, EIG_SMALL_THREADS).total;
+    if (ep.method != EIG_MODE_TOP1 && eig_small(CPLX, n) && ep.smem_bytes <= EIG_SMALL_SMEM)
+      return eig_launch<CPLX, NS, EIG_SMALL_THREADS>(n, ep, w, s, ad, small > ep.smem_bytes ? small : ep.smem_bytes,
+                                                     1);
+  }
   bool in_smem;
   size_t smem = eig_smem_bytes(CPLX, n, &in_smem);
   if (ep.smem_bytes > smem) smem = ep.smem_bytes;  // a batch whose smaller patches fit shared memory
@@ -1384,14 +1428,7 @@ static cudaError_t eig_ns(int n, const EigParams& ep, const PatchWork& w, cudaSt
       flags |= 2;
     }
   }
-  auto kern = (ep.method == PD_METHOD_ADAPTIVE || ep.method == EIG_MODE_FULL) ? k_eig<CPLX, NS, true>
-                                                                               : k_eig<CPLX, NS, false>;
-  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (err != cudaSuccess) return err;
-  pd_adaptive a{};
-  if (ad) a = *ad;
-  PD_TIMED(ep.method == EIG_MODE_TOP1 ? "eig_mc" : "eig", s, kern<<<w.count, EIG_THREADS, smem, s>>>(n, ep, w, flags, a));
-  return cudaGetLastError();
+  return eig_launch<CPLX, NS, EIG_THREADS>(n, ep, w, s, ad, smem, flags);
 }
 
 template <bool CPLX>

@@ -104,6 +104,10 @@ constexpr int EIG_MODE_FULL = 101;
 cudaError_t launch_eig(bool cplx, int n, const EigParams& ep, const PatchWork& w, cudaStream_t s,
                        const pd_adaptive* ad = nullptr);
 size_t eig_smem_bytes(bool cplx, int n, bool* in_smem);
+// whether k_eig runs patches of n frames in small (128-thread) CTAs, and the
+// dynamic shared memory its launch for them takes
+bool eig_small(bool cplx, int n);
+size_t eig_launch_smem(bool cplx, int n);
 
 // pd_sub.cu: subspace solver of the hard-threshold rule (mixed precision path)
 bool sub_supported(bool cplx, int n, int rows);
