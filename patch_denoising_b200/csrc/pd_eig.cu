@@ -371,14 +371,32 @@ struct TriInfo {
   float gl, gu, pivmin, abstol, tnorm;
 };
 
-// Eigenvalues at indices idx[0..cnt) into out[]; warps take entries.
+// Eigenvalues at indices idx[0..cnt) into out[]. A few: a warp each, by
+// 33-way multisection. Many (whole spectra): a thread each, by bisection with
+// the same stopping rule (the Sturm counts of all eigenvalues then run side by
+// side instead of 32 points of one eigenvalue per round).
 template <int TH>
 __device__ void cta_eigs(const float* d, const float* e2, int n, const TriInfo& ti, const int* idx,
                          float* out, int cnt) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int q = warp; q < cnt; q += (TH / 32)) {
-    const float v = warp_kth(d, e2, n, idx[q], ti.gl, ti.gu, ti.pivmin, ti.abstol);
-    if (lane == 0) out[q] = v;
+  if (cnt > 2 * (TH / 32)) {
+    for (int q = threadIdx.x; q < cnt; q += TH) {
+      const int k = idx[q];
+      float lo = ti.gl, hi = ti.gu;
+      for (int it = 0; it < 64; ++it) {
+        const float tol = fmaxf(2.f * FLT_EPSILON * fmaxf(fabsf(lo), fabsf(hi)), ti.abstol);
+        if (!(hi - lo > tol)) break;
+        const float x = 0.5f * (lo + hi);
+        if (sturm_count(d, e2, n, x, ti.pivmin) <= k) lo = x;
+        else hi = x;
+      }
+      out[q] = 0.5f * (lo + hi);
+    }
+  } else {
+    for (int q = warp; q < cnt; q += (TH / 32)) {
+      const float v = warp_kth(d, e2, n, idx[q], ti.gl, ti.gu, ti.pivmin, ti.abstol);
+      if (lane == 0) out[q] = v;
+    }
   }
   __syncthreads();
 }
