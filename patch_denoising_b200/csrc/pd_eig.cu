@@ -1,4 +1,6 @@
-// Per-patch Hermitian eigensolver and threshold rules (one CTA per patch).
+// Per-patch Hermitian eigensolver and threshold rules (one CTA per patch: 512
+// threads, or 128 threads and four CTAs per SM for patches of at most 128
+// frames whose layout fits a quarter of shared memory).
 //
 //  1. The packed lower Gram C = Xc^H Xc (n = frames) is staged in shared memory
 //     when it fits (else worked on in place in global memory) and scaled by
@@ -6,15 +8,18 @@
 //  2. Householder reduction to real symmetric tridiagonal form T = Q^H C Q
 //     (H_j = I - tau_j v_j v_j^H, v_j stored below the subdiagonal), the
 //     classical unblocked algorithm (Golub & Van Loan, sec. 8.3.1).
-//  3. Eigenvalues of T at requested indices by Sturm-count multisection: one
-//     warp evaluates 32 points per round, shrinking the bracket 33x.
+//  3. Eigenvalues of T at requested indices by Sturm counts: a few by
+//     multisection (one warp evaluates 32 points per round, shrinking the
+//     bracket 33x), a whole spectrum by bisection with a thread per eigenvalue.
 //  4. The reference threshold rule of the method, evaluated in FP64 on the
 //     eigenvalues (space_time/lowrank.py: MP-PCA :42-63, Hybrid :104-119,
 //     Raw/NORDIC :170-184, Optimal :379-407), gives maxidx, noise_var and the
 //     active components with their synthesis coefficients.
 //  5. Eigenvectors of T for the active components by the twisted factorisation
-//     (Parlett & Dhillon, 1997), re-orthogonalised inside eigenvalue clusters,
-//     then back-transformed by the reflectors: eigenvectors of C.
+//     (Parlett & Dhillon, 1997), re-orthogonalised inside eigenvalue clusters
+//     (block classical Gram-Schmidt for whole bulks), then back-transformed by
+//     the reflectors, a warp applying each reflector to a group of vectors:
+//     eigenvectors of C.
 #include <float.h>
 
 #include "pd_common.cuh"
