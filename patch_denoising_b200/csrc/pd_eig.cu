@@ -1108,11 +1108,21 @@ __global__ void __launch_bounds__(TH, TH >= 512 ? 1 : 4) k_eig(int n, EigParams 
         r = i;
       }
     }
+    // the running element stays in a register (no reload of what this thread
+    // stored one step earlier); z[i] holds D-(i) until it is overwritten
     z[r] = 1.f;
-    for (int i = r + 1; i < n; ++i) z[i] = -(e[i - 1] / z[i]) * z[i - 1];
-    for (int i = r - 1; i >= 0; --i) z[i] = -(e[i] / Dp[i]) * z[i + 1];
-    float s2 = 0.f;
-    for (int i = 0; i < n; ++i) s2 += z[i] * z[i];
+    float s2 = 1.f, zv = 1.f;
+    for (int i = r + 1; i < n; ++i) {
+      zv = -(e[i - 1] / z[i]) * zv;
+      z[i] = zv;
+      s2 += zv * zv;
+    }
+    zv = 1.f;
+    for (int i = r - 1; i >= 0; --i) {
+      zv = -(e[i] / Dp[i]) * zv;
+      z[i] = zv;
+      s2 += zv * zv;
+    }
     const float inv = rsqrtf(s2);
     for (int i = 0; i < n; ++i) z[i] *= inv;
   }
