@@ -28,7 +28,10 @@ from patch_denoising_b200.space_time import AdaptiveDenoiser
 
 pytestmark = pytest.mark.gpu
 
-ADAPTIVE_TIE = {"fp32": 5e-3, "mixed": 2e-2}
+# singular values carry half the relative error of the split-bf16 Gram's
+# eigenvalues (at most 1.9e-3 on the parity volumes, test_mixed_tie_bound.py):
+# the mixed band is 1e-2, as the other rules'
+ADAPTIVE_TIE = {"fp32": 5e-3, "mixed": 1e-2}
 # rel-L2 bounds against the FP64 oracle (float32 LAPACK singular values move
 # the search's result by ~1e-7; the Gram route's spectrum is less accurate)
 ADAPTIVE_TOL = {"fp32": 1e-4, "mixed": 1e-3}
